@@ -1,0 +1,139 @@
+// aarbf_internal.h -- context state and kernel launchers shared by the library's sources.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/aarbf.h"
+#include "aarbf_device.cuh"
+
+namespace aarbf {
+
+// Grow-only device buffer.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  cudaError_t reserve(size_t want) {
+    if (want <= bytes) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    size_t alloc = want < 256 ? 256 : want;
+    cudaError_t e = cudaMalloc(&ptr, alloc);
+    if (e == cudaSuccess) bytes = alloc;
+    return e;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Everything the tracking / marching / splat kernels read about a built scene.
+struct SceneView {
+  const float4* rec0;  // x, y, z, r_eval
+  const float4* w4;    // a^3, pow(rgb, 2.2) a^3
+  const float4* xyzw;  // sorted particles (attribute normalised)
+  const float* rgeom;  // bounds radius, -1 = skipped by the bounds program
+  const Node* nodes;
+  const float4* tf_color;
+  const float* tf_density;
+  uint64_t n;
+  uint32_t ppl;
+  uint32_t nleaves;
+  uint32_t root;  // child code of the root
+  int nc, nd;
+  float root_lo[3], root_hi[3];
+  float eps;      // absolute slack used by conservative culling tests
+  int per_particle_radius;
+};
+
+struct RenderLaunch {
+  SceneView s;
+  uint32_t accum_id, frame_id, spp, flags;
+  float ambient;
+  float light[3];
+  float cam_pos[3], cam_d00[3], cam_du[3], cam_dv[3];
+  float rbf_radius, unit, density_gain, jitter_x, jitter_y;
+  float aabb_min[3], aabb_max[3];
+  const uchar4* noise;
+  int noise_w, noise_h;
+  int width, height;
+  float4* accum;
+  float4* image;
+  uint32_t* status;
+  int traversal;
+  float splat_rmax;                // largest splat radius of the scene
+  unsigned long long* counters;    // count mode: [particles on traversed segments, node visits]
+};
+
+// launchers (defined in the .cu files)
+cudaError_t launch_domain_reduce(const float4* p, uint64_t n, float* d_partial, int nblocks,
+                                 cudaStream_t st);
+cudaError_t launch_hilbert_keys(const float4* p, uint64_t n, const float* dom, uint64_t* keys,
+                                uint32_t* perm, cudaStream_t st);
+cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt, uint32_t* vals_alt,
+                             uint64_t n, int key_bits, uint32_t* hist, size_t hist_words,
+                             cudaStream_t st, bool* result_in_alt);
+size_t radix_sort_hist_words(uint64_t n);
+cudaError_t launch_tie_check(const uint64_t* keys, uint64_t n, uint32_t* flag, cudaStream_t st);
+cudaError_t launch_orderable_component(const float4* p, const uint32_t* perm, uint64_t n, int comp,
+                                       uint64_t* out, cudaStream_t st);
+cudaError_t launch_hilbert_keys_perm(const float4* p, const uint32_t* perm, uint64_t n, const float* dom,
+                                     uint64_t* keys, cudaStream_t st);
+cudaError_t launch_gather_normalize(const float4* in, const float* radii_in, const uint32_t* perm,
+                                    uint64_t n, float amin, float amax, float4* out,
+                                    float* radii_out, cudaStream_t st);
+cudaError_t launch_prepass(const float4* xyzw, const float* radii, uint64_t n, const float4* tf_color,
+                           int nc, const float* tf_radius, int nr, float rbf_radius, float4* rec0,
+                           float4* w4, float* rgeom, cudaStream_t st);
+cudaError_t launch_karras(const uint64_t* sorted_keys, uint64_t n, uint32_t ppl, uint32_t nleaves,
+                          Node* nodes, uint32_t* leaf_parent, cudaStream_t st);
+cudaError_t launch_refit(const float4* rec0, const float* rgeom, uint64_t n, uint32_t ppl,
+                         uint32_t nleaves, Node* nodes, const uint32_t* leaf_parent, uint32_t* counters,
+                         float* leaf_box, float* root_box, cudaStream_t st);
+cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st);
+cudaError_t launch_splat(const RenderLaunch& L, cudaStream_t st);
+cudaError_t launch_taa(const float4* image, const float4* prev, float4* taa, uint32_t* bgra, int w,
+                       int h, int disable, cudaStream_t st);
+
+}  // namespace aarbf
+
+struct aarbf_ctx {
+  int device = 0;
+  std::string last_error;
+  // input frame
+  aarbf::DevBuf in_xyzw, in_radii;
+  uint64_t n = 0;
+  bool has_radii = false;
+  // domain
+  float dom[8] = {0, 0, 0, 1, 1, 1, 0, 1};
+  bool has_domain = false;
+  // sort
+  aarbf::DevBuf keys, keys_alt, perm, perm_alt, hist, tmp_keys, flag;
+  // sorted scene
+  aarbf::DevBuf xyzw, radii, rec0, w4, rgeom, nodes, leaf_parent, counters, leaf_box, root_box;
+  aarbf::DevBuf sorted_keys;  // Hilbert keys in sorted order
+  uint32_t ppl = 1, nleaves = 0;
+  float rbf_radius = 0.0f;
+  bool built = false;
+  float root_box_host[6] = {0, 0, 0, 0, 0, 0};
+  // transfer functions
+  aarbf::DevBuf tf_color, tf_radius, tf_density;
+  int nc = 0, nr = 0, nd = 0;
+  bool has_tf = false;
+  // noise atlas
+  aarbf::DevBuf noise;
+  int noise_w = 0, noise_h = 0;
+  // framebuffers owned by the context
+  aarbf::DevBuf fb_accum, fb_image;
+  int fb_w = 0, fb_h = 0;
+  // status word
+  aarbf::DevBuf status;
+  float max_radius = 0.0f;
+};

@@ -1,0 +1,189 @@
+// lbvh.cu -- the reference's bounds program (deviceCodeBounds.hlsl:29-82) turned into an LBVH
+// builder: per-particle shading prepass, Karras (HPG 2012) radix tree over the leaf clusters'
+// Hilbert keys, and a bottom-up refit that computes the leaf boxes exactly as GenRBFBounds
+// does and unions them upwards with atomic arrival counters.
+#include "aarbf_internal.h"
+
+namespace aarbf {
+
+namespace {
+
+inline unsigned blocks_for(uint64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// radius (deviceCodeRBF.hlsl:349-351, deviceCodeBounds.hlsl:59) and the per-particle any-hit
+// weights (deviceCodeRBF.hlsl:366-376), evaluated once per particle instead of once per hit
+__global__ void k_prepass(const float4* __restrict__ xyzw, const float* __restrict__ radii, uint64_t n,
+                          const float4* __restrict__ tf_color, int nc, const float* __restrict__ tf_radius,
+                          int nr, float rbf_radius, float4* __restrict__ rec0, float4* __restrict__ w4,
+                          float* __restrict__ rgeom) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 p = __ldg(xyzw + i);
+  float rp = tex1(tf_radius, nr, p.w);
+  float base = radii ? __ldg(radii + i) : rbf_radius;
+  float r = base * rp;
+  float4 col = tex4(tf_color, nc, p.w);
+  rgeom[i] = (rp == 0.0f) ? -1.0f : r;
+  if (col.w == 0.0f) {
+    rec0[i] = make_float4(p.x, p.y, p.z, 0.0f);
+    w4[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  } else {
+    float a3 = (col.w * col.w) * col.w;
+    rec0[i] = make_float4(p.x, p.y, p.z, r);
+    w4[i] = make_float4(a3, dpow(col.x, 2.2f) * a3, dpow(col.y, 2.2f) * a3, dpow(col.z, 2.2f) * a3);
+  }
+}
+
+__device__ __forceinline__ int delta(const uint64_t* __restrict__ keys, uint32_t ppl, int64_t L, int64_t i,
+                                     int64_t j) {
+  if (j < 0 || j >= L) return -1;
+  uint64_t a = __ldg(keys + (uint64_t)i * ppl), b = __ldg(keys + (uint64_t)j * ppl);
+  uint64_t x = a ^ b;
+  if (x == 0) return 64 + __clz((int)((uint32_t)i ^ (uint32_t)j));
+  return __clzll((long long)x);
+}
+
+// leaf l's key is the key of its first particle; equal keys are ordered by leaf index
+__global__ void k_karras(const uint64_t* __restrict__ keys, uint32_t ppl, uint32_t nleaves, Node* nodes,
+                         uint32_t* leaf_parent) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t L = nleaves;
+  if (i >= L - 1) return;
+  int d = (delta(keys, ppl, L, i, i + 1) - delta(keys, ppl, L, i, i - 1)) >= 0 ? 1 : -1;
+  int dmin = delta(keys, ppl, L, i, i - d);
+  int64_t lmax = 2;
+  while (delta(keys, ppl, L, i, i + lmax * d) > dmin) lmax *= 2;
+  int64_t l = 0;
+  for (int64_t t = lmax / 2; t >= 1; t /= 2)
+    if (delta(keys, ppl, L, i, i + (l + t) * d) > dmin) l += t;
+  int64_t j = i + l * d;
+  int dnode = delta(keys, ppl, L, i, j);
+  int64_t s = 0, step = l;
+  do {
+    step = (step + 1) >> 1;
+    if (delta(keys, ppl, L, i, i + (s + step) * d) > dnode) s += step;
+  } while (step > 1);
+  int64_t g = i + s * d + (d < 0 ? -1 : 0);
+  int64_t lo = i < j ? i : j, hi = i < j ? j : i;
+  uint32_t left = (lo == g) ? ((uint32_t)g | kLeafBit) : (uint32_t)g;
+  uint32_t right = (hi == g + 1) ? ((uint32_t)(g + 1) | kLeafBit) : (uint32_t)(g + 1);
+  nodes[i].d.x = left;
+  nodes[i].d.y = right;
+  nodes[i].d.w = 0u;
+  if (i == 0) nodes[0].d.z = 0xffffffffu;
+  if (left & kLeafBit) leaf_parent[left & ~kLeafBit] = (uint32_t)i;
+  else nodes[left].d.z = (uint32_t)i;
+  if (right & kLeafBit) leaf_parent[right & ~kLeafBit] = (uint32_t)i;
+  else nodes[right].d.z = (uint32_t)i;
+}
+
+__device__ __forceinline__ void write_slot(Node* node, int slot, const float* lo, const float* hi) {
+  float* f = reinterpret_cast<float*>(node) + 6 * slot;
+  f[0] = lo[0]; f[1] = lo[1]; f[2] = lo[2];
+  f[3] = hi[0]; f[4] = hi[1]; f[5] = hi[2];
+}
+
+__device__ __forceinline__ void read_union(const Node* node, float* lo, float* hi) {
+  const float* f = reinterpret_cast<const float*>(node);
+  float v[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) v[k] = __ldcg(f + k);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = fminf(v[a], v[6 + a]);
+    hi[a] = fmaxf(v[3 + a], v[9 + a]);
+  }
+}
+
+// one thread per leaf: GenRBFBounds (deviceCodeBounds.hlsl:45-81), then walk up the tree; the
+// second child to arrive at an internal node computes its box.
+__global__ void k_refit(const float4* __restrict__ rec0, const float* __restrict__ rgeom, uint64_t n,
+                        uint32_t ppl, uint32_t nleaves, Node* nodes, const uint32_t* __restrict__ leaf_parent,
+                        uint32_t* counters, float* __restrict__ leaf_box, float* __restrict__ root_box) {
+  uint64_t l = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (l >= nleaves) return;
+  const float inf = __int_as_float(0x7f800000);
+  float lo[3] = {inf, inf, inf}, hi[3] = {-inf, -inf, -inf};
+  for (uint32_t k = 0; k < ppl; ++k) {
+    uint64_t i = l * ppl + k;
+    if (i >= n) break;
+    float r = __ldg(rgeom + i);
+    if (r < 0.0f) continue;  // radiusPercent == 0
+    float4 p = __ldg(rec0 + i);
+    lo[0] = fminf(lo[0], p.x - r); lo[1] = fminf(lo[1], p.y - r); lo[2] = fminf(lo[2], p.z - r);
+    hi[0] = fmaxf(hi[0], p.x + r); hi[1] = fmaxf(hi[1], p.y + r); hi[2] = fmaxf(hi[2], p.z + r);
+  }
+  if (lo[0] > hi[0] || lo[1] > hi[1] || lo[2] > hi[2]) {
+    const float nan = __int_as_float(0x7fc00000);
+    lo[0] = lo[1] = lo[2] = hi[0] = hi[1] = hi[2] = nan;
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    leaf_box[6 * l + a] = lo[a];
+    leaf_box[6 * l + 3 + a] = hi[a];
+  }
+  if (nleaves == 1) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      root_box[a] = lo[a];
+      root_box[3 + a] = hi[a];
+    }
+    return;
+  }
+  uint32_t child = (uint32_t)l | kLeafBit;
+  uint32_t parent = leaf_parent[l];
+  for (int guard = 0; guard < 256; ++guard) {
+    Node* pn = nodes + parent;
+    int slot = (pn->d.x == child) ? 0 : 1;
+    write_slot(pn, slot, lo, hi);
+    __threadfence();
+    if (atomicAdd(counters + parent, 1u) == 0u) return;
+    __threadfence();
+    read_union(pn, lo, hi);
+    uint32_t up = pn->d.z;
+    if (up == 0xffffffffu) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        root_box[a] = lo[a];
+        root_box[3 + a] = hi[a];
+      }
+      return;
+    }
+    child = parent;
+    parent = up;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_prepass(const float4* xyzw, const float* radii, uint64_t n, const float4* tf_color, int nc,
+                           const float* tf_radius, int nr, float rbf_radius, float4* rec0, float4* w4,
+                           float* rgeom, cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  k_prepass<<<blocks_for(n, 256), 256, 0, st>>>(xyzw, radii, n, tf_color, nc, tf_radius, nr, rbf_radius, rec0,
+                                                w4, rgeom);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_karras(const uint64_t* sorted_keys, uint64_t n, uint32_t ppl, uint32_t nleaves, Node* nodes,
+                          uint32_t* leaf_parent, cudaStream_t st) {
+  (void)n;
+  if (nleaves < 2) return cudaSuccess;
+  k_karras<<<blocks_for(nleaves - 1, 256), 256, 0, st>>>(sorted_keys, ppl, nleaves, nodes, leaf_parent);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_refit(const float4* rec0, const float* rgeom, uint64_t n, uint32_t ppl, uint32_t nleaves,
+                         Node* nodes, const uint32_t* leaf_parent, uint32_t* counters, float* leaf_box,
+                         float* root_box, cudaStream_t st) {
+  if (!nleaves) return cudaSuccess;
+  if (nleaves > 1) {
+    cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(uint32_t) * (nleaves - 1), st);
+    if (e != cudaSuccess) return e;
+  }
+  k_refit<<<blocks_for(nleaves, 256), 256, 0, st>>>(rec0, rgeom, n, ppl, nleaves, nodes, leaf_parent, counters,
+                                                   leaf_box, root_box);
+  return cudaGetLastError();
+}
+
+}  // namespace aarbf

@@ -1,0 +1,576 @@
+// render.cu -- ParticleRBFRayGen + ParticleTracker + ParticleRBFIntersection/AnyHit
+// (deviceCodeRBF.hlsl:40-389) as one CUDA kernel.
+//
+// The reference issues one zero-length ray per tracking step and lets the RT cores find every
+// leaf box containing the step point. Here the density at a step point is the exact sum over
+// particles with |x - p| < r, accumulated in 64-bit fixed point (2^-40 units), so the result does
+// not depend on the order particles are visited. Two traversal strategies give identical bits:
+//   STAGED: a ray is cut into segments; one BVH traversal per segment stages every particle whose
+//           (slightly inflated) sphere meets the segment, with its ray-parameter interval, in
+//           shared memory; each step then only scans the staged list. A segment whose candidates
+//           overflow the buffer is halved; below a minimum length the steps fall back to POINT.
+//   POINT:  one stack-based BVH point query per step (the reference's shape).
+#include "aarbf_internal.h"
+
+namespace aarbf {
+
+namespace {
+
+constexpr int kBlock = 128;  // 16 x 8 pixel tile per block
+
+struct Ray {
+  float3 o, d;
+  float tmin, tmax;
+};
+
+struct Sample {
+  int count;
+  long long a0, a1, a2, a3;
+};
+
+__device__ __forceinline__ void sample_clear(Sample& s) {
+  s.count = 0;
+  s.a0 = s.a1 = s.a2 = s.a3 = 0;
+}
+
+__device__ __forceinline__ void eval_particle(const SceneView& s, uint32_t i, float3 x, Sample& acc) {
+  float4 r = __ldg(s.rec0 + i);
+  float dx = r.x - x.x, dy = r.y - x.y, dz = r.z - x.z;
+  float dist = sqrtf((dx * dx + dy * dy) + dz * dz);
+  if (!(dist < r.w)) return;
+  float q = (dist * 3.0f) / r.w;  // evaluate_rbf, sigma = 3 (sharedCode.h:137-140)
+  float rho = dexp(-0.5f * (q * q));
+  float4 w = __ldg(s.w4 + i);
+  acc.count += 1;
+  acc.a0 += fix40(rho * w.x);
+  acc.a1 += fix40(rho * w.y);
+  acc.a2 += fix40(rho * w.z);
+  acc.a3 += fix40(rho * w.w);
+}
+
+__device__ __forceinline__ void eval_leaf(const SceneView& s, uint32_t leaf, float3 x, Sample& acc) {
+  uint64_t b = (uint64_t)leaf * s.ppl;
+  uint64_t e = b + s.ppl;
+  if (e > s.n) e = s.n;
+  for (uint64_t i = b; i < e; ++i) eval_particle(s, (uint32_t)i, x, acc);
+}
+
+__device__ __forceinline__ bool inside(float lx, float ly, float lz, float hx, float hy, float hz, float3 x) {
+  return x.x >= lx && x.x <= hx && x.y >= ly && x.y <= hy && x.z >= lz && x.z <= hz;
+}
+
+// POINT: every leaf whose box contains x, then the exact particle test
+__device__ void point_query(const SceneView& s, float3 x, Sample& acc, uint32_t* status) {
+  sample_clear(acc);
+  if (s.nleaves == 0) return;
+  if (!inside(s.root_lo[0], s.root_lo[1], s.root_lo[2], s.root_hi[0], s.root_hi[1], s.root_hi[2], x)) return;
+  if (s.root & kLeafBit) {
+    eval_leaf(s, s.root & ~kLeafBit, x, acc);
+    return;
+  }
+  uint32_t stack[kStackSize];
+  int sp = 0;
+  uint32_t node = s.root;
+  while (true) {
+    const Node* nd = s.nodes + node;
+    float4 a = __ldg(&nd->a), b = __ldg(&nd->b), c = __ldg(&nd->c);
+    uint2 ch = __ldg(reinterpret_cast<const uint2*>(&nd->d));
+    bool h0 = inside(a.x, a.y, a.z, a.w, b.x, b.y, x);
+    bool h1 = inside(b.z, b.w, c.x, c.y, c.z, c.w, x);
+    if (h0 && (ch.x & kLeafBit)) {
+      eval_leaf(s, ch.x & ~kLeafBit, x, acc);
+      h0 = false;
+    }
+    if (h1 && (ch.y & kLeafBit)) {
+      eval_leaf(s, ch.y & ~kLeafBit, x, acc);
+      h1 = false;
+    }
+    if (h0 && h1) {
+      if (sp == kStackSize) {
+        atomicOr(status, kStatusStackOverflow);
+        return;
+      }
+      stack[sp++] = ch.y;
+      node = ch.x;
+    } else if (h0) {
+      node = ch.x;
+    } else if (h1) {
+      node = ch.y;
+    } else {
+      if (sp == 0) break;
+      node = stack[--sp];
+    }
+  }
+}
+
+// slab test of a (slack-inflated) box against the ray segment [t0, t1]
+__device__ __forceinline__ bool seg_box(float lx, float ly, float lz, float hx, float hy, float hz, float3 o,
+                                        float3 inv, float t0, float t1, float eps) {
+  float ax = (lx - eps - o.x) * inv.x, bx = (hx + eps - o.x) * inv.x;
+  float ay = (ly - eps - o.y) * inv.y, by = (hy + eps - o.y) * inv.y;
+  float az = (lz - eps - o.z) * inv.z, bz = (hz + eps - o.z) * inv.z;
+  float tn = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), t0));
+  float tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), t1));
+  return tn <= tf;
+}
+
+// Per-thread staged candidate buffer, structure-of-arrays in shared memory:
+// entry j of thread t lives at [j * kBlock + t].
+template <int CAP>
+struct Stager {
+  uint32_t* idx;
+  float* lo;
+  float* hi;
+  int ncand;       // -1: point-query mode for the current segment
+  float seg_end;   // the staged segment covers steps with t < seg_end
+  float len;       // current segment length
+  float len_min, len_max;
+  float rb_enter, rb_exit;  // ray interval inside the inflated root box
+  float3 inv;
+
+  __device__ void init(const SceneView& s, const Ray& ray, float unit, char* smem) {
+    const int t = threadIdx.x;
+    idx = reinterpret_cast<uint32_t*>(smem) + t;
+    lo = reinterpret_cast<float*>(smem + sizeof(uint32_t) * CAP * kBlock) + t;
+    hi = reinterpret_cast<float*>(smem + (sizeof(uint32_t) + sizeof(float)) * CAP * kBlock) + t;
+    ncand = 0;
+    seg_end = -__int_as_float(0x7f800000);
+    len_min = unit * 0.25f;
+    len_max = unit * 64.0f;
+    len = unit * 16.0f;
+    inv = make_float3(1.0f / ray.d.x, 1.0f / ray.d.y, 1.0f / ray.d.z);
+    float e = s.eps * 4.0f;
+    float ax = (s.root_lo[0] - e - ray.o.x) * inv.x, bx = (s.root_hi[0] + e - ray.o.x) * inv.x;
+    float ay = (s.root_lo[1] - e - ray.o.y) * inv.y, by = (s.root_hi[1] + e - ray.o.y) * inv.y;
+    float az = (s.root_lo[2] - e - ray.o.z) * inv.z, bz = (s.root_hi[2] + e - ray.o.z) * inv.z;
+    rb_enter = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz));
+    rb_exit = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
+    if (s.nleaves == 0 || !(rb_enter <= rb_exit)) {
+      rb_enter = __int_as_float(0x7f800000);
+      rb_exit = -__int_as_float(0x7f800000);
+    }
+  }
+
+  __device__ __forceinline__ bool push(uint32_t i, float a, float b) {
+    if (ncand == CAP) return false;
+    idx[ncand * kBlock] = i;
+    lo[ncand * kBlock] = a;
+    hi[ncand * kBlock] = b;
+    ++ncand;
+    return true;
+  }
+
+  // stage all particles whose inflated sphere meets [t0, t1]; false on buffer overflow
+  __device__ bool stage(const SceneView& s, const Ray& ray, float t0, float t1, uint32_t* status) {
+    ncand = 0;
+    const float eps = s.eps;
+    uint32_t stack[kStackSize];
+    int sp = 0;
+    uint32_t node = s.root;
+    const bool root_leaf = (s.root & kLeafBit) != 0;
+    uint32_t leaves[2];
+    while (true) {
+      int nl = 0;
+      uint32_t next0 = 0xffffffffu, next1 = 0xffffffffu;
+      if (root_leaf) {
+        leaves[nl++] = s.root & ~kLeafBit;
+      } else {
+        const Node* nd = s.nodes + node;
+        float4 a = __ldg(&nd->a), b = __ldg(&nd->b), c = __ldg(&nd->c);
+        uint2 ch = __ldg(reinterpret_cast<const uint2*>(&nd->d));
+        bool h0 = seg_box(a.x, a.y, a.z, a.w, b.x, b.y, ray.o, inv, t0, t1, eps);
+        bool h1 = seg_box(b.z, b.w, c.x, c.y, c.z, c.w, ray.o, inv, t0, t1, eps);
+        if (h0) {
+          if (ch.x & kLeafBit) leaves[nl++] = ch.x & ~kLeafBit;
+          else next0 = ch.x;
+        }
+        if (h1) {
+          if (ch.y & kLeafBit) leaves[nl++] = ch.y & ~kLeafBit;
+          else next1 = ch.y;
+        }
+      }
+      for (int k = 0; k < nl; ++k) {
+        uint64_t b0 = (uint64_t)leaves[k] * s.ppl;
+        uint64_t e0 = b0 + s.ppl;
+        if (e0 > s.n) e0 = s.n;
+        for (uint64_t i = b0; i < e0; ++i) {
+          float4 r = __ldg(s.rec0 + i);
+          if (!(r.w > 0.0f)) continue;
+          float vx = r.x - ray.o.x, vy = r.y - ray.o.y, vz = r.z - ray.o.z;
+          float tc = (vx * ray.d.x + vy * ray.d.y) + vz * ray.d.z;
+          float wx = vx - tc * ray.d.x, wy = vy - tc * ray.d.y, wz = vz - tc * ray.d.z;
+          float h2 = (wx * wx + wy * wy) + wz * wz;
+          float R = r.w * (1.0f + 0x1p-10f) + eps;
+          float R2 = R * R;
+          if (h2 > R2) continue;
+          float half = sqrtf(R2 - h2) + eps;
+          float a = tc - half, b = tc + half;
+          if (b < t0 || a > t1) continue;
+          if (!push((uint32_t)i, a, b)) return false;
+        }
+      }
+      if (root_leaf) return true;
+      if (next0 != 0xffffffffu && next1 != 0xffffffffu) {
+        if (sp == kStackSize) {
+          atomicOr(status, kStatusStackOverflow);
+          return true;
+        }
+        stack[sp++] = next1;
+        node = next0;
+      } else if (next0 != 0xffffffffu) {
+        node = next0;
+      } else if (next1 != 0xffffffffu) {
+        node = next1;
+      } else {
+        if (sp == 0) return true;
+        node = stack[--sp];
+      }
+    }
+  }
+
+  // make sure the step at t is covered by the staged segment
+  __device__ void cover(const SceneView& s, const Ray& ray, float t, uint32_t* status) {
+    if (t < seg_end) return;
+    if (t < rb_enter) {  // before the scene: nothing can be hit
+      ncand = 0;
+      seg_end = rb_enter;
+      return;
+    }
+    if (t > rb_exit) {  // past the scene
+      ncand = 0;
+      seg_end = __int_as_float(0x7f800000);
+      return;
+    }
+    for (int guard = 0; guard < 64; ++guard) {
+      float te = t + len;
+      if (!(te > t)) break;
+      if (stage(s, ray, t, te, status)) {
+        seg_end = te;
+        len = fminf(len * 2.0f, len_max);
+        return;
+      }
+      len = len * 0.5f;
+      if (len < len_min) break;
+    }
+    // dense or degenerate: point queries until t + len_min
+    ncand = -1;
+    float te = t + len_min;
+    seg_end = (te > t) ? te : t;
+    len = len_min * 4.0f;
+  }
+
+  __device__ __forceinline__ void sample(const SceneView& s, float t, float3 x, Sample& acc, uint32_t* status) {
+    if (ncand < 0) {
+      point_query(s, x, acc, status);
+      return;
+    }
+    sample_clear(acc);
+    for (int j = 0; j < ncand; ++j) {
+      float a = lo[j * kBlock], b = hi[j * kBlock];
+      if (t < a || t > b) continue;
+      eval_particle(s, idx[j * kBlock], x, acc);
+    }
+  }
+};
+
+// Count mode (roofline accounting, not timed): the particles whose sphere meets the traversed
+// segment [t0, t1] of a ray (exact test, no slack) and the BVH nodes a segment query visits.
+__device__ void count_segment(const RenderLaunch& L, const Ray& ray, float t0, float t1) {
+  const SceneView& s = L.s;
+  if (s.nleaves == 0 || !(t1 >= t0)) return;
+  const float3 inv = make_float3(1.0f / ray.d.x, 1.0f / ray.d.y, 1.0f / ray.d.z);
+  unsigned long long parts = 0, visits = 0;
+  uint32_t stack[kStackSize];
+  int sp = 0;
+  uint32_t node = s.root;
+  const bool root_leaf = (s.root & kLeafBit) != 0;
+  while (true) {
+    uint32_t leaves[2];
+    int nl = 0;
+    uint32_t n0 = 0xffffffffu, n1 = 0xffffffffu;
+    if (root_leaf) {
+      leaves[nl++] = s.root & ~kLeafBit;
+    } else {
+      ++visits;
+      const Node* nd = s.nodes + node;
+      float4 a = __ldg(&nd->a), b = __ldg(&nd->b), c = __ldg(&nd->c);
+      uint2 ch = __ldg(reinterpret_cast<const uint2*>(&nd->d));
+      if (seg_box(a.x, a.y, a.z, a.w, b.x, b.y, ray.o, inv, t0, t1, 0.0f)) {
+        if (ch.x & kLeafBit) leaves[nl++] = ch.x & ~kLeafBit;
+        else n0 = ch.x;
+      }
+      if (seg_box(b.z, b.w, c.x, c.y, c.z, c.w, ray.o, inv, t0, t1, 0.0f)) {
+        if (ch.y & kLeafBit) leaves[nl++] = ch.y & ~kLeafBit;
+        else n1 = ch.y;
+      }
+    }
+    for (int k = 0; k < nl; ++k) {
+      uint64_t b0 = (uint64_t)leaves[k] * s.ppl, e0 = b0 + s.ppl;
+      if (e0 > s.n) e0 = s.n;
+      for (uint64_t i = b0; i < e0; ++i) {
+        float4 r = __ldg(s.rec0 + i);
+        if (!(r.w > 0.0f)) continue;
+        float vx = r.x - ray.o.x, vy = r.y - ray.o.y, vz = r.z - ray.o.z;
+        float tc = (vx * ray.d.x + vy * ray.d.y) + vz * ray.d.z;
+        float wx = vx - tc * ray.d.x, wy = vy - tc * ray.d.y, wz = vz - tc * ray.d.z;
+        float h2 = (wx * wx + wy * wy) + wz * wz;
+        float R2 = r.w * r.w;
+        if (h2 >= R2) continue;
+        float half = sqrtf(R2 - h2);
+        if (tc + half < t0 || tc - half > t1) continue;
+        ++parts;
+      }
+    }
+    if (root_leaf) break;
+    if (n0 != 0xffffffffu && n1 != 0xffffffffu) {
+      if (sp == kStackSize) break;
+      stack[sp++] = n1;
+      node = n0;
+    } else if (n0 != 0xffffffffu) {
+      node = n0;
+    } else if (n1 != 0xffffffffu) {
+      node = n1;
+    } else {
+      if (sp == 0) break;
+      node = stack[--sp];
+    }
+  }
+  atomicAdd(L.counters + 0, parts);
+  atomicAdd(L.counters + 1, visits);
+}
+
+struct Tracker {
+  int i;
+  float random;
+  uint32_t rng;
+  float4 albedo;
+  float t;
+  float lhs;
+  bool shadow;
+  bool marching;
+};
+
+__device__ __forceinline__ float sample_density(const RenderLaunch& L, float D) {
+  if (L.flags & kFlagDensityLinear) return fminf(D * L.density_gain, 1.0f);
+  return tex1(L.s.tf_density, L.s.nd, D);
+}
+
+__device__ __forceinline__ float3 sample_color(const RenderLaunch& L, const Sample& acc, float D) {
+  if (L.flags & kFlagVisualizeAttributes) {
+    const float g = 1.0f / 2.2f;
+    float c0 = (float)acc.a1 * kFixInv, c1 = (float)acc.a2 * kFixInv, c2 = (float)acc.a3 * kFixInv;
+    return make_float3(dpow(c0 / D, g), dpow(c1 / D, g), dpow(c2 / D, g));
+  }
+  float4 c = tex4(L.s.tf_color, L.s.nc, D);
+  return make_float3(c.x, c.y, c.z);
+}
+
+template <int CAP>
+__device__ __forceinline__ void do_sample(const RenderLaunch& L, Stager<CAP>& st, const Ray& ray, float t, float3 x,
+                                          Sample& acc) {
+  if (L.traversal == AARBF_TRAVERSAL_POINT) {
+    point_query(L.s, x, acc, L.status);
+  } else {
+    st.cover(L.s, ray, t, L.status);
+    st.sample(L.s, t, x, acc, L.status);
+  }
+}
+
+// stochasticTracking (deviceCodeRBF.hlsl:141-203)
+template <int CAP>
+__device__ void track_delta(const RenderLaunch& L, Tracker& tr, const Ray& ray, bool from_entry, char* smem) {
+  Stager<CAP> st;
+  st.init(L.s, ray, L.unit, smem);
+  if (!from_entry) tr.t = ray.tmin;
+  for (; tr.i < kMaxDepth; ++tr.i) {
+    float u = lcg_f(tr.rng);
+    float step = (dlog(1.0f - u) / 1.0f) * L.unit;
+    tr.t = tr.t - step;
+    if (tr.t >= ray.tmax) return;
+    float3 x = make_float3(ray.o.x + tr.t * ray.d.x, ray.o.y + tr.t * ray.d.y, ray.o.z + tr.t * ray.d.z);
+    Sample acc;
+    do_sample<CAP>(L, st, ray, tr.t, x, acc);
+    if (acc.count == 0) continue;
+    float D = (float)acc.a0 * kFixInv;
+    float density = sample_density(L, D);
+    if (lcg_f(tr.rng) < density / 1.0f) {
+      float3 c = sample_color(L, acc, D);
+      tr.albedo = make_float4(c.x, c.y, c.z, 1.0f);
+      return;
+    }
+  }
+}
+
+// stochasticMarching (deviceCodeRBF.hlsl:67-139)
+template <int CAP>
+__device__ void track_march(const RenderLaunch& L, Tracker& tr, const Ray& ray, char* smem) {
+  Stager<CAP> st;
+  st.init(L.s, ray, L.unit, smem);
+  float rhs = -dlog(1.0f - tr.random * 0.99f);
+  for (; tr.i < kMaxDepth; ++tr.i) {
+    tr.t = tr.t + L.unit;
+    if (tr.t >= ray.tmax) return;
+    float3 x = make_float3(ray.o.x + tr.t * ray.d.x, ray.o.y + tr.t * ray.d.y, ray.o.z + tr.t * ray.d.z);
+    Sample acc;
+    do_sample<CAP>(L, st, ray, tr.t, x, acc);
+    float D = (float)acc.a0 * kFixInv;
+    if (!(acc.count > 0 && D > 0.0f)) continue;
+    float density = sample_density(L, D);
+    tr.lhs = tr.lhs + density;
+    if (tr.lhs > rhs && !tr.shadow) {
+      float3 c = sample_color(L, acc, D);
+      tr.albedo = make_float4(c.x, c.y, c.z, 1.0f);
+      return;
+    }
+    if (tr.shadow) {
+      tr.albedo.w = tr.albedo.w + (1.0f - dexp(-density));
+      if (tr.albedo.w >= 1.0f) {
+        tr.albedo.w = 1.0f;
+        return;
+      }
+    }
+  }
+}
+
+template <int CAP>
+__device__ __forceinline__ void track(const RenderLaunch& L, Tracker& tr, const Ray& ray, bool from_entry,
+                                      char* smem) {
+  if (tr.marching) track_march<CAP>(L, tr, ray, smem);
+  else track_delta<CAP>(L, tr, ray, from_entry, smem);
+}
+
+// ParticleRBFRayGen body for one sample (deviceCodeRBF.hlsl:206-324)
+template <int CAP>
+__device__ float4 raygen_sample(const RenderLaunch& L, uint32_t frame, int px, int py, float& noise, char* smem) {
+  uint32_t rng = pixel_seed(frame, (uint32_t)px, (uint32_t)py, (uint32_t)L.width);
+  float sx = ((float)px + 0.5f + L.jitter_x) / (float)L.width;
+  float sy = ((float)py + 0.5f + L.jitter_y) / (float)L.height;
+  float3 rt = make_float3(L.aabb_max[0] + 2.0f * L.rbf_radius, L.aabb_max[1] + 2.0f * L.rbf_radius,
+                          L.aabb_max[2] + 2.0f * L.rbf_radius);
+  float3 lb = make_float3(L.aabb_min[0] - 2.0f * L.rbf_radius, L.aabb_min[1] - 2.0f * L.rbf_radius,
+                          L.aabb_min[2] - 2.0f * L.rbf_radius);
+  Ray ray;
+  ray.o = make_float3(L.cam_pos[0], L.cam_pos[1], L.cam_pos[2]);
+  float3 dir = make_float3((L.cam_d00[0] + sx * L.cam_du[0]) + sy * L.cam_dv[0],
+                           (L.cam_d00[1] + sx * L.cam_du[1]) + sy * L.cam_dv[1],
+                           (L.cam_d00[2] + sx * L.cam_du[2]) + sy * L.cam_dv[2]);
+  ray.d = normalize3(dir);
+  ray.tmin = 0.0f;
+  ray.tmax = 10000.0f;
+  float tenter, texit;
+  aabb_clip(ray.o, ray.d, lb, rt, ray.tmin, ray.tmax, tenter, texit);
+
+  Tracker tr;
+  const bool blue = (L.flags & kFlagBlueNoise) != 0;
+  float r0;
+  if (blue) {
+    uint32_t gx = frame % 8u, gy = (frame / 8u) % 16u;
+    uint32_t cx = gx * 256u + (uint32_t)px % 256u, cy = gy * 256u + (uint32_t)py % 256u;
+    r0 = 0.0f;
+    if (L.noise && (int)cx < L.noise_w && (int)cy < L.noise_h)
+      r0 = (float)L.noise[(size_t)cy * (size_t)L.noise_w + cx].x / 255.0f;
+    tr.marching = true;
+    tr.rng = 0u;
+  } else {
+    r0 = lcg_f(rng);
+    tr.marching = false;
+    tr.rng = rng;
+  }
+  float r1 = lcg_f(rng);
+  float r2 = lcg_f(rng);
+  tr.i = 0;
+  tr.lhs = 0.0f;
+  tr.random = r0;
+  tr.albedo = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  tr.shadow = false;
+  noise = r0;
+  float4 color = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (tenter < texit) {
+    ray.tmax = texit;
+    tr.t = tenter + L.unit * r1;
+    const bool from_entry = (L.flags & kFlagTrackFromEntry) != 0;
+    const float t_start = (blue || from_entry) ? tr.t : ray.tmin;
+    track<CAP>(L, tr, ray, from_entry, smem);
+    float4 albedo = tr.albedo;
+    float t = tr.t;
+    if (L.counters) count_segment(L, ray, t_start, fminf(t, ray.tmax));
+    float vis = 1.0f;
+    if (albedo.w > 0.0f && L.ambient != 1.0f) {
+      Ray sr;
+      sr.o = make_float3(ray.o.x + ray.d.x * t, ray.o.y + ray.d.y * t, ray.o.z + ray.d.z * t);
+      sr.d = make_float3(L.light[0], L.light[1], L.light[2]);
+      sr.tmin = 0.0f;
+      sr.tmax = 10000.0f;
+      float ste, stx;
+      aabb_clip(sr.o, sr.d, lb, rt, sr.tmin, sr.tmax, ste, stx);
+      sr.tmax = stx;
+      tr.albedo = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      tr.lhs = 0.0f;
+      tr.shadow = true;
+      tr.t = blue ? -L.unit * r2 : 0.0f;
+      const float ts0 = tr.t;
+      track<CAP>(L, tr, sr, false, smem);
+      vis = 1.0f - tr.albedo.w;
+      if (L.counters) count_segment(L, sr, fmaxf(ts0, 0.0f), fminf(tr.t, sr.tmax));
+    }
+    if (albedo.w == 1.0f) {
+      color.x = (albedo.x * vis) * (1.0f - L.ambient) + albedo.x * L.ambient;
+      color.y = (albedo.y * vis) * (1.0f - L.ambient) + albedo.y * L.ambient;
+      color.z = (albedo.z * vis) * (1.0f - L.ambient) + albedo.z * L.ambient;
+      color.w = 1.0f;
+    }
+  }
+  return over4(color, make_float4(0.0f, 0.0f, 0.0f, 1.0f));
+}
+
+template <int CAP>
+__global__ void __launch_bounds__(kBlock) k_render(const RenderLaunch L) {
+  extern __shared__ __align__(16) char smem[];
+  const int px = blockIdx.x * 16 + (threadIdx.x & 15);
+  const int py = blockIdx.y * 8 + (threadIdx.x >> 4);
+  if (px >= L.width || py >= L.height) return;
+  const size_t ofs = (size_t)px + (size_t)L.width * (size_t)py;
+  float4 prev = L.accum[ofs];
+  float4 fin = prev;
+  float noise = 0.0f;
+  const uint32_t spp = L.spp ? L.spp : 1u;
+  for (uint32_t k = 0; k < spp; ++k) {
+    uint32_t frame = (L.frame_id + k) & 0xffffu;
+    uint32_t aid = (L.accum_id + k) & 0xffffu;
+    float4 c = raygen_sample<CAP>(L, frame, px, py, noise, smem);
+    // running mean, deviceCodeRBF.hlsl:326-328
+    float fa = (float)aid;
+    float wa = 1.0f / fa, wb = (float)((int)aid - 1) / fa;
+    fin.x = wa * c.x + wb * prev.x;
+    fin.y = wa * c.y + wb * prev.y;
+    fin.z = wa * c.z + wb * prev.z;
+    fin.w = wa * c.w + wb * prev.w;
+    prev = fin;
+  }
+  L.accum[ofs] = fin;
+  if (L.flags & kFlagShowNoise) fin = make_float4(noise, noise, noise, 1.0f);
+  L.image[ofs] = fin;
+}
+
+template <int CAP>
+cudaError_t launch_cap(const RenderLaunch& L, cudaStream_t st) {
+  size_t smem = (sizeof(uint32_t) + 2 * sizeof(float)) * CAP * kBlock;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_render<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  dim3 grid((L.width + 15) / 16, (L.height + 7) / 8);
+  k_render<CAP><<<grid, kBlock, smem, st>>>(L);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st) {
+  if (L.width <= 0 || L.height <= 0) return cudaSuccess;
+  return launch_cap<32>(L, st);
+}
+
+}  // namespace aarbf

@@ -1,0 +1,256 @@
+// splat.cu -- ParticleSplatRayGen / ParticleSplatIntersection / ParticleSplatAnyHit
+// (deviceCodeSplat.hlsl:29-193): Knoll/Wald-style slab-sorted splatting.
+//
+// The ray is cut into slabs of width unit (PARTICLE_BUFFER_SIZE / 8 = 1 in integer arithmetic,
+// deviceCodeSplat.hlsl:80). A slab keeps at most 15 samples; which 15 the reference keeps depends
+// on hardware traversal order, here they are the 15 smallest (t, particle index). Candidates of
+// a run of slabs are staged once per BVH traversal in shared memory and sorted; a slab with more
+// than the buffer holds is resolved by a streaming top-15 traversal of that slab alone.
+#include "aarbf_internal.h"
+
+namespace aarbf {
+
+namespace {
+
+constexpr int kBlock = 128;
+constexpr int kCap = 32;
+constexpr int kKeep = 15;  // PARTICLE_BUFFER_SIZE, deviceCodeSplat.hlsl:36
+
+__device__ __forceinline__ bool seg_box(float lx, float ly, float lz, float hx, float hy, float hz, float3 o,
+                                        float3 inv, float t0, float t1, float pad) {
+  float ax = (lx - pad - o.x) * inv.x, bx = (hx + pad - o.x) * inv.x;
+  float ay = (ly - pad - o.y) * inv.y, by = (hy + pad - o.y) * inv.y;
+  float az = (lz - pad - o.z) * inv.z, bz = (hz + pad - o.z) * inv.z;
+  float tn = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), t0));
+  float tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), t1));
+  return tn <= tf;
+}
+
+__device__ __forceinline__ float splat_radius(const RenderLaunch& L, uint32_t i) {
+  float rg = __ldg(L.s.rgeom + i);
+  if (rg < 0.0f) return 0.0f;  // radiusmap == 0: not splatted
+  return (L.flags & kFlagSplatParticleRadius) ? rg : L.rbf_radius;
+}
+
+// ParticleSplatIntersection test (deviceCodeSplat.hlsl:165-179) without the slab condition;
+// returns t = |c - o| when accepted, -1 otherwise
+__device__ __forceinline__ float splat_t(const RenderLaunch& L, uint32_t i, float3 o, float3 d) {
+  float r = splat_radius(L, i);
+  if (!(r > 0.0f)) return -1.0f;
+  float4 c = __ldg(L.s.xyzw + i);
+  float vx = c.x - o.x, vy = c.y - o.y, vz = c.z - o.z;
+  float t = sqrtf((vx * vx + vy * vy) + vz * vz);
+  float sx = o.x + t * d.x, sy = o.y + t * d.y, sz = o.z + t * d.z;
+  float ox = c.x - sx, oy = c.y - sy, oz = c.z - sz;
+  if (!(((ox * ox + oy * oy) + oz * oz) < r * r)) return -1.0f;
+  return t;
+}
+
+__device__ __forceinline__ bool less_ti(float ta, uint32_t ia, float tb, uint32_t ib) {
+  return ta < tb || (ta == tb && ia < ib);
+}
+
+// visit every particle of every leaf whose padded box meets [t0, t1]; f(i) returns false to stop
+template <class F>
+__device__ bool traverse(const RenderLaunch& L, float3 o, float3 inv, float t0, float t1, float pad, F&& f) {
+  const SceneView& s = L.s;
+  if (s.nleaves == 0) return true;
+  uint32_t stack[kStackSize];
+  int sp = 0;
+  uint32_t node = s.root;
+  const bool root_leaf = (s.root & kLeafBit) != 0;
+  while (true) {
+    uint32_t leaves[2];
+    int nl = 0;
+    uint32_t n0 = 0xffffffffu, n1 = 0xffffffffu;
+    if (root_leaf) {
+      leaves[nl++] = s.root & ~kLeafBit;
+    } else {
+      const Node* nd = s.nodes + node;
+      float4 a = __ldg(&nd->a), b = __ldg(&nd->b), c = __ldg(&nd->c);
+      uint2 ch = __ldg(reinterpret_cast<const uint2*>(&nd->d));
+      if (seg_box(a.x, a.y, a.z, a.w, b.x, b.y, o, inv, t0, t1, pad)) {
+        if (ch.x & kLeafBit) leaves[nl++] = ch.x & ~kLeafBit;
+        else n0 = ch.x;
+      }
+      if (seg_box(b.z, b.w, c.x, c.y, c.z, c.w, o, inv, t0, t1, pad)) {
+        if (ch.y & kLeafBit) leaves[nl++] = ch.y & ~kLeafBit;
+        else n1 = ch.y;
+      }
+    }
+    for (int k = 0; k < nl; ++k) {
+      uint64_t b0 = (uint64_t)leaves[k] * s.ppl, e0 = b0 + s.ppl;
+      if (e0 > s.n) e0 = s.n;
+      for (uint64_t i = b0; i < e0; ++i)
+        if (!f((uint32_t)i)) return false;
+    }
+    if (root_leaf) return true;
+    if (n0 != 0xffffffffu && n1 != 0xffffffffu) {
+      if (sp == kStackSize) {
+        atomicOr(L.status, kStatusStackOverflow);
+        return true;
+      }
+      stack[sp++] = n1;
+      node = n0;
+    } else if (n0 != 0xffffffffu) {
+      node = n0;
+    } else if (n1 != 0xffffffffu) {
+      node = n1;
+    } else {
+      if (sp == 0) return true;
+      node = stack[--sp];
+    }
+  }
+}
+
+__device__ __forceinline__ float4 shade_sample(const RenderLaunch& L, uint32_t id, float t, float3 o, float3 d,
+                                               float atten) {
+  float4 P = __ldg(L.s.xyzw + id);
+  float r = splat_radius(L, id);
+  float X0 = o.x + d.x * t, X1 = o.y + d.y * t, X2 = o.z + d.z * t;
+  float dx = X0 - P.x, dy = X1 - P.y, dz = X2 - P.z;
+  float dist = sqrtf((dx * dx + dy * dy) + dz * dz);
+  float q = (dist * 3.0f) / r;
+  float drbf = dexp(-0.5f * (q * q));
+  float4 col;
+  if (L.flags & kFlagVisualizeAttributes) {
+    col = tex4(L.s.tf_color, L.s.nc, P.w);
+    drbf = tex1(L.s.tf_density, L.s.nd, drbf);
+    col.w = col.w * drbf;
+  } else {
+    float4 c = tex4(L.s.tf_color, L.s.nc, drbf);
+    col = make_float4(c.x, c.y, c.z, tex1(L.s.tf_density, L.s.nd, drbf));
+  }
+  col.w = col.w * atten;
+  return col;
+}
+
+__global__ void __launch_bounds__(kBlock) k_splat(const RenderLaunch L, float pad) {
+  __shared__ float sh_t[kCap][kBlock];
+  __shared__ uint32_t sh_i[kCap][kBlock];
+  const int tid = threadIdx.x;
+  const int px = blockIdx.x * 16 + (tid & 15);
+  const int py = blockIdx.y * 8 + (tid >> 4);
+  if (px >= L.width || py >= L.height) return;
+  float sx = ((float)px + 0.5f + L.jitter_x) / (float)L.width;
+  float sy = ((float)py + 0.5f + L.jitter_y) / (float)L.height;
+  float3 rt = make_float3(L.aabb_max[0] + L.rbf_radius, L.aabb_max[1] + L.rbf_radius, L.aabb_max[2] + L.rbf_radius);
+  float3 lb = make_float3(L.aabb_min[0] - L.rbf_radius, L.aabb_min[1] - L.rbf_radius, L.aabb_min[2] - L.rbf_radius);
+  float3 o = make_float3(L.cam_pos[0], L.cam_pos[1], L.cam_pos[2]);
+  float3 d = normalize3(make_float3((L.cam_d00[0] + sx * L.cam_du[0]) + sy * L.cam_dv[0],
+                                    (L.cam_d00[1] + sx * L.cam_du[1]) + sy * L.cam_dv[1],
+                                    (L.cam_d00[2] + sx * L.cam_du[2]) + sy * L.cam_dv[2]));
+  float tenter, texit;
+  aabb_clip(o, d, lb, rt, 0.0f, 10000.0f, tenter, texit);
+  float4 res = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (tenter < texit) {
+    const float3 inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    const float spacing = (float)(kKeep / 8) * L.unit;
+    const float atten = dexp(-L.unit * (float)(kKeep / 8));
+    float tslab = 0.0f;
+    int run = 16;  // slabs staged per traversal
+    int guard = 0;
+    while (tslab < texit && guard < (1 << 24)) {
+      ++guard;
+      if (res.w > 0.99f) break;
+      // skip slabs that end before the entry point
+      float tmax0 = fminf(texit, tslab + spacing);
+      if (!(tmax0 > tenter)) {
+        tslab = tslab + spacing;
+        continue;
+      }
+      // stage the next `run` slabs
+      float s_end = tslab;
+      int nslab = 0;
+      for (; nslab < run && s_end < texit; ++nslab) s_end = s_end + spacing;
+      float lo = fmaxf(tenter, tslab), hi = fminf(texit, s_end);
+      int cnt = 0;
+      bool ok = traverse(L, o, inv, lo, hi, pad, [&](uint32_t i) {
+        float t = splat_t(L, i, o, d);
+        if (t < 0.0f || !(t >= lo && t < hi)) return true;
+        if (cnt == kCap) return false;
+        sh_t[cnt][tid] = t;
+        sh_i[cnt][tid] = i;
+        ++cnt;
+        return true;
+      });
+      if (!ok && nslab > 1) {
+        run = nslab / 2;
+        continue;
+      }
+      if (ok) {
+        // insertion sort by (t, id)
+        for (int a = 1; a < cnt; ++a) {
+          float ta = sh_t[a][tid];
+          uint32_t ia = sh_i[a][tid];
+          int b = a - 1;
+          while (b >= 0 && less_ti(ta, ia, sh_t[b][tid], sh_i[b][tid])) {
+            sh_t[b + 1][tid] = sh_t[b][tid];
+            sh_i[b + 1][tid] = sh_i[b][tid];
+            --b;
+          }
+          sh_t[b + 1][tid] = ta;
+          sh_i[b + 1][tid] = ia;
+        }
+        int cur = 0;
+        for (int k = 0; k < nslab; ++k) {
+          if (!(tslab < texit)) break;
+          if (res.w > 0.99f) break;
+          float tmin = fmaxf(tenter, tslab), tmax = fminf(texit, tslab + spacing);
+          if (tmax > tenter) {
+            while (cur < cnt && sh_t[cur][tid] < tmin) ++cur;
+            int taken = 0;
+            while (cur < cnt && taken < kKeep && sh_t[cur][tid] < tmax) {
+              float4 col = shade_sample(L, sh_i[cur][tid], sh_t[cur][tid], o, d, atten);
+              res = over4(res, col);
+              ++cur;
+              ++taken;
+            }
+          }
+          tslab = tslab + spacing;
+        }
+        if (run < 64) run *= 2;
+      } else {
+        // a single slab with more candidates than the buffer: streaming top-15 of the slab
+        float tmin = fmaxf(tenter, tslab), tmax = fminf(texit, tslab + spacing);
+        float kt[kKeep];
+        uint32_t ki[kKeep];
+        int kc = 0;
+        traverse(L, o, inv, tmin, tmax, pad, [&](uint32_t i) {
+          float t = splat_t(L, i, o, d);
+          if (t < 0.0f || !(t >= tmin && t < tmax)) return true;
+          if (kc == kKeep && !less_ti(t, i, kt[kKeep - 1], ki[kKeep - 1])) return true;
+          int b = (kc < kKeep) ? kc : kKeep - 1;
+          if (kc < kKeep) ++kc;
+          while (b > 0 && less_ti(t, i, kt[b - 1], ki[b - 1])) {
+            kt[b] = kt[b - 1];
+            ki[b] = ki[b - 1];
+            --b;
+          }
+          kt[b] = t;
+          ki[b] = i;
+          return true;
+        });
+        for (int k = 0; k < kc; ++k) res = over4(res, shade_sample(L, ki[k], kt[k], o, d, atten));
+        tslab = tslab + spacing;
+        run = 1;
+      }
+    }
+  }
+  res = over4(res, make_float4(0.0f, 0.0f, 0.0f, 1.0f));
+  L.image[(size_t)px + (size_t)L.width * (size_t)py] = res;
+}
+
+}  // namespace
+
+cudaError_t launch_splat(const RenderLaunch& L, cudaStream_t st) {
+  if (L.width <= 0 || L.height <= 0) return cudaSuccess;
+  // a splat sample lies within its particle's radius of the centre, and the centre lies in
+  // its leaf box: padding every box by twice the largest splat radius keeps the test robust
+  float pad = 2.0f * L.splat_rmax + 4.0f * L.s.eps;
+  dim3 grid((L.width + 15) / 16, (L.height + 7) / 8);
+  k_splat<<<grid, kBlock, 0, st>>>(L, pad);
+  return cudaGetLastError();
+}
+
+}  // namespace aarbf

@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Benchmark: Mrays/s of attribute-aware Gaussian-RBF particle-volume rendering on B200.
+
+Workload (one step): the 10M-particle scene of the benchmark configuration (64 anisotropic
+Gaussian clusters + 5% uniform background, radii log-uniform [0.002, 0.02], 256-entry RGBA fp32
+transfer function with 4 opacity peaks), delta tracking with one shadow ray per sample,
+1920x1080, 16 samples per pixel, step unit 0.001 (0.5 x min radius), density scale 50.
+A ray is one primary camera sample including its shadow ray. Inputs are larger than L2 (the
+particle records and BVH nodes alone exceed 1 GB), so no L2 flush is inserted between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value      : rays of all ranks / max-over-ranks device time of the K timed steps (scene resident)
+e2e        : the same metric through the public C ABI with host buffers: per step the particle
+             upload (pinned host -> device), the build (Hilbert sort + LBVH), the render and the
+             image read-back are inside the timed region
+roofline   : algorithmic bytes of one render launch (20 B per particle whose sphere meets a
+             traversed ray segment + 64 B per BVH node visit + 48 B per pixel of framebuffer
+             traffic) / measured launch time, against the measured HBM copy bandwidth
+cpu_baseline: the oracle (C restatement of the reference's device code, OpenMP over pixels) on a
+             bounded, evenly spread sample of the same frame's pixels, on this host's cores
+Multi-GPU: replicas (each rank renders its own frames of the replicated scene; weak scaling).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "attribute-aware-rbfs_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "Mrays/s at 10M particles 1080p vs plain & CPU at equal RMSE; fwd+bwd ms/iter"
+UNIT = "Mrays/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--particles", type=int, default=10_000_000)
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--spp", type=int, default=16)
+    ap.add_argument("--unit", type=float, default=0.001)
+    ap.add_argument("--density-scale", type=float, default=50.0)
+    ap.add_argument("--traversal", type=int, default=0, help="0 staged, 1 point query")
+    ap.add_argument("--ppl", type=int, default=1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
+            int(os.environ.get("WORLD_SIZE", "1")))
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per render launch from the committed ncu summary (scaled there to this
+    workload), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "render_traffic.json")) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.idx)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for k, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(k)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_scene(args):
+    from aarbf import scenes
+    sc = scenes.config_clusters(args.particles, seed=2)
+    cm, rm, dm = scenes.tf_four_peaks()
+    return sc, (cm, rm, dm)
+
+
+def domain_of(xyzw):
+    d = np.empty(8, np.float32)
+    d[0:3] = xyzw[:, :3].min(0)
+    d[3:6] = xyzw[:, :3].max(0)
+    d[6] = xyzw[:, 3].min()
+    d[7] = xyzw[:, 3].max()
+    return d
+
+
+def params_for(args, dom, rmax, frame_id=0):
+    from aarbf import scenes
+    return scenes.native_params(scenes.orbit_camera(), args.width, args.height, rmax, args.unit,
+                                args.density_scale, dom, spp=args.spp, frame_id=frame_id,
+                                traversal=args.traversal)
+
+
+def cpu_scene(args, sc, tf, dom, rbf_radius):
+    import oracle.oracle as orc
+    return orc.build_scene(sc.xyzw, sc.radii, dom, args.ppl, rbf_radius, tf)[0]
+
+
+def cpu_sample(args, scene, rp, target_s, threads):
+    """Render an evenly spread sample of the frame's pixels with the oracle; returns
+    (Mrays/s, rays, seconds, description)."""
+    import oracle.oracle as orc
+    p = orc.params_from(rp)
+    p.spp = 1
+    W, H = args.width, args.height
+    tile = 8
+    accum = np.zeros((H, W, 4), np.float32)
+    image = np.zeros((H, W, 4), np.float32)
+
+    def run(ntiles_side):
+        xs = np.linspace(0, W - tile, ntiles_side).astype(int)
+        ys = np.linspace(0, H - tile, ntiles_side).astype(int)
+        t0 = time.perf_counter()
+        for y in ys:
+            for x in xs:
+                scene.render(p, W, H, accum=accum, threads=threads, image=image,
+                             region=(int(x), int(x) + tile, int(y), int(y) + tile))
+        dt = time.perf_counter() - t0
+        return len(xs) * len(ys) * tile * tile, dt
+
+    rays, dt = run(4)
+    side = 4
+    while dt < target_s * 0.4 and side < 64:
+        side = min(64, int(side * max(1.5, (target_s / max(dt, 1e-3)) ** 0.5)))
+        rays, dt = run(side)
+    desc = (f"{side}x{side} tiles of {tile}x{tile} pixels spread evenly over the {W}x{H} frame, 1 spp "
+            f"({rays} rays) of the same scene, camera and estimator")
+    return rays / dt / 1e6, rays, dt, desc
+
+
+def run_reference(args):
+    """--impl reference: the oracle port of the reference's device code on the host cores."""
+    rank, _, world = dist_env()
+    if world > 1 and rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    sc, tf = make_scene(args)
+    dom = domain_of(sc.xyzw)
+    rp = params_for(args, dom, float(sc.radii.max()))
+    scene = cpu_scene(args, sc, tf, dom, rp.rbf_radius)
+    vals = []
+    for k in range(args.warmup + args.steps):
+        v, rays, dt, desc = cpu_sample(args, scene, rp, max(2.0, args.cpu_seconds / 2), threads)
+        if k >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32",
+        "data": "synthetic (seeded generator at the benchmark configuration's sizes and distributions)",
+        "config": config_dict(args),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "vs_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(args):
+    return {"workload": f"clusters_{args.particles // 1_000_000}M_{args.width}x{args.height}_{args.spp}spp_delta_tracking",
+            "particles": args.particles, "width": args.width, "height": args.height, "spp": args.spp,
+            "estimator": "delta tracking + shadow ray", "unit": args.unit, "density_scale": args.density_scale,
+            "traversal": "staged" if args.traversal == 0 else "point", "particles_per_leaf": args.ppl,
+            "l2": "inputs_larger_than_l2", "parallelism": f"replicas{args.gpus}"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    import aarbf
+
+    rank, local_rank, world = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    sc, tf = make_scene(args)
+    dom = domain_of(sc.xyzw)
+    rmax = float(sc.radii.max())
+    ctx = aarbf.Context(local_rank)
+    stream = torch.cuda.Stream(device=dev)
+    sp = stream.cuda_stream
+    xyzw_pin = torch.from_numpy(sc.xyzw).pin_memory()
+    radii_pin = torch.from_numpy(sc.radii).pin_memory()
+    ctx.set_domain(dom)
+    ctx.set_transfer_functions_f32(*tf)
+    ctx.set_particles(xyzw_pin, radii_pin, stream=sp)
+    t_b0 = time.perf_counter()
+    ctx.build(rmax, args.ppl, stream=sp)
+    build_s = time.perf_counter() - t_b0
+    W, H, S = args.width, args.height, args.spp
+    accum = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)
+    image = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)
+
+    def step(k):
+        rp = params_for(args, dom, rmax, frame_id=(k * S + rank * 7919) & 0xFFFF)
+        ctx.render(rp, W, H, accum, image, stream=sp)
+
+    for k in range(args.warmup):
+        step(k)
+    ctx.sync(sp)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for k in range(args.steps):
+        step(args.warmup + k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ctx.sync(sp)
+    t = e0.elapsed_time(e1) / 1e3
+    tt = torch.tensor([t], device=dev)
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    t = float(tt.item())
+    rays = W * H * S * args.steps * world
+    value = rays / t / 1e6
+    ms_per_step = t / args.steps * 1e3
+
+    # roofline accounting: one counted launch (untimed)
+    rp = params_for(args, dom, rmax, frame_id=0)
+    parts, visits = ctx.render_count(rp, W, H, accum, image, stream=sp)
+    alg_bytes = 20 * parts + 64 * visits + 48 * W * H
+    launch_s = t / args.steps
+    achieved = alg_bytes / launch_s / 1e9
+    peak, peak_kind = measured_peak()
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        host_img = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+        k_e2e = max(1, min(args.steps, 3))
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for k in range(k_e2e):
+            ctx.set_particles(xyzw_pin, radii_pin, stream=sp)
+            ctx.build(rmax, args.ppl, stream=sp)
+            rpk = params_for(args, dom, rmax, frame_id=(k * S) & 0xFFFF)
+            ctx.render(rpk, W, H, accum, image, stream=sp)
+            ctx.memcpy(host_img, image, H * W * 16, stream=sp)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        te = f0.elapsed_time(f1) / 1e3
+        te_t = torch.tensor([te], device=dev)
+        if world > 1:
+            dist.all_reduce(te_t, op=dist.ReduceOp.MAX)
+        te = float(te_t.item())
+        e2e = {"value": W * H * S * k_e2e * world / te / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": int(sc.xyzw.nbytes + sc.radii.nbytes), "d2h_bytes_per_step": H * W * 16,
+               "steps": k_e2e, "ms_per_step": te / k_e2e * 1e3}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        scene = cpu_scene(args, sc, tf, dom, rp.rbf_radius)
+        v, r_cpu, dt, desc = cpu_sample(args, scene, rp, args.cpu_seconds, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc,
+               "seconds": round(dt, 2)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generator at the benchmark configuration's sizes and distributions)",
+            "config": config_dict(args),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": profiled_traffic(), "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": alg_bytes, "particles_on_segments": parts,
+                         "node_visits": visits},
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": args.steps,
+            "build_ms": build_s * 1e3,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

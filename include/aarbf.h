@@ -1,0 +1,214 @@
+/*
+ * aarbf.h -- C ABI of the B200 attribute-aware Gaussian-RBF particle-volume renderer.
+ *
+ * This is the drop-in boundary for the reference's GPU path (gprt-org/attribute-aware-rbfs):
+ * the GPRT program registration and launches of hostCode.cpp (bounds compute program,
+ * hardware BVH build/refit, the RBF ray-generation program with its intersection/any-hit
+ * programs, the splat ray-generation program, the CompositeGui TAA pass). Each entry point
+ * below names the reference interface it replaces (file:line in the reference tree).
+ *
+ * Conventions
+ *  - Plain pointers and sizes; no C++ or torch types. All functions return aarbf_status and
+ *    never abort; aarbf_last_error() gives a message for the last failing call on a context.
+ *  - A context is bound to one CUDA device and is not internally locked: use one context per
+ *    host thread. GPU work is enqueued on the caller's stream (`stream` is a cudaStream_t;
+ *    NULL = the legacy default stream). aarbf_render* do not synchronise.
+ *  - Particle and transfer-function inputs may be host or device pointers (detected).
+ *    Render targets are caller-owned device pointers (float4 per pixel, row-major,
+ *    offset = x + width * y as in deviceCodeRBF.hlsl:210) or NULL for context-owned ones.
+ */
+#ifndef AARBF_H
+#define AARBF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AARBF_VERSION_MAJOR 0
+#define AARBF_VERSION_MINOR 1
+
+typedef enum aarbf_status {
+  AARBF_OK = 0,
+  AARBF_ERR_INVALID_ARGUMENT = 1,
+  AARBF_ERR_OUT_OF_MEMORY = 2,
+  AARBF_ERR_CUDA = 3,
+  AARBF_ERR_DEVICE_LIMIT = 4, /* a device-side cap was hit (traversal stack, loop cap) */
+  AARBF_ERR_NOT_READY = 5,    /* e.g. render before build */
+  AARBF_ERR_IO = 6,
+  AARBF_ERR_UNSUPPORTED = 7
+} aarbf_status;
+
+typedef struct aarbf_ctx aarbf_ctx;
+
+/* Render flags: PushConstants booleans (sharedCode.h:37-40) plus native-mode switches. */
+enum {
+  AARBF_FLAG_BLUE_NOISE = 1u << 0,           /* enableBlueNoise -> stochastic marching */
+  AARBF_FLAG_SHOW_NOISE = 1u << 1,           /* showNoise */
+  AARBF_FLAG_VISUALIZE_ATTRIBUTES = 1u << 2, /* visualizeAttributes (reference default: on) */
+  AARBF_FLAG_TRACK_FROM_ENTRY = 1u << 3,     /* native: delta tracking starts at tenter + unit*xi */
+  AARBF_FLAG_DENSITY_LINEAR = 1u << 4,       /* native: density = min(D * density_gain, 1) */
+  AARBF_FLAG_SPLAT_PARTICLE_RADIUS = 1u << 5 /* native: splats use the per-particle radius */
+};
+
+/* Traversal strategies of the render kernel (identical results). */
+enum {
+  AARBF_TRAVERSAL_STAGED = 0, /* per-ray segments: candidates staged in shared memory */
+  AARBF_TRAVERSAL_POINT = 1   /* one BVH point query per tracking step (reference shape) */
+};
+
+/*
+ * Per-launch parameters. Mirrors PushConstants (sharedCode.h:33-74) and the RayGenData record
+ * (sharedCode.h:108-117): accumID/frameID are taken modulo 2^16 like the reference's uint16.
+ * spp > 1 renders spp consecutive frames (frameID+k, accumID+k) in one launch; the result is
+ * bit-identical to spp launches of one frame each.
+ */
+typedef struct aarbf_params {
+  uint32_t accum_id;
+  uint32_t frame_id;
+  uint32_t spp;
+  uint32_t flags;
+  float light_azimuth, light_elevation, light_ambient;
+  float cam_pos[3], cam_dir00[3], cam_du[3], cam_dv[3];
+  float rbf_radius;  /* global radius (per-particle radii multiply nothing into it) */
+  float unit;        /* delta-tracking / marching step unit */
+  float aabb_min[3]; /* RayGenData.globalAABBMin / Max: the space-time box */
+  float aabb_max[3];
+  float density_gain; /* AARBF_FLAG_DENSITY_LINEAR: density scale * unit */
+  float jitter_x, jitter_y; /* sub-pixel camera jitter in pixels (0 = reference) */
+  int32_t traversal;        /* AARBF_TRAVERSAL_* */
+  int32_t reserved[3];
+} aarbf_params;
+
+/* ---- context -------------------------------------------------------------------------- */
+
+/* replaces gprtContextCreate (hostCode.cpp:280-281): bind a context to CUDA device `device` */
+aarbf_status aarbf_create(aarbf_ctx **out, int device);
+/* replaces the gprt*Destroy calls (hostCode.cpp:834-848) */
+aarbf_status aarbf_destroy(aarbf_ctx *ctx);
+const char *aarbf_last_error(const aarbf_ctx *ctx);
+const char *aarbf_status_string(aarbf_status s);
+aarbf_status aarbf_get_version(int *major, int *minor);
+/* waits for the stream, then reports (and clears) device-side error bits */
+aarbf_status aarbf_sync(aarbf_ctx *ctx, void *stream);
+
+/* ---- particles and domain --------------------------------------------------------------- */
+
+/* Upload one frame of particles: float4 (x, y, z, attribute) x n, as importParticles
+ * (importParticles.h:8-31) yields them; replaces the particle buffer upload
+ * (hostCode.cpp:759-763). radii: optional per-particle radius (n floats) or NULL. */
+aarbf_status aarbf_set_particles(aarbf_ctx *ctx, const float *xyzw, uint64_t n, const float *radii,
+                                 void *stream);
+
+/* Space-time domain used to quantise Hilbert keys and normalise attributes
+ * (hostCode.cpp:183-193, :227-250). dom = {minx,miny,minz,maxx,maxy,maxz,attr_min,attr_max}. */
+aarbf_status aarbf_set_domain(aarbf_ctx *ctx, const float *dom);
+/* Reduce frames on the device into a running domain (initialise dom with aarbf_domain_init). */
+aarbf_status aarbf_domain_init(float *dom);
+aarbf_status aarbf_domain_accumulate(aarbf_ctx *ctx, const float *xyzw, uint64_t n, float *dom,
+                                     void *stream);
+
+/* ---- transfer functions (hostCode.cpp:355-365, :416-436, :524-572) ------------------------ */
+
+/* 8-bit textures exactly as the reference uploads them (R8G8B8A8_SRGB): colormap RGBA x nc,
+ * radiusmap and densitymap use their R channel (RGBA x nr / x nd). */
+aarbf_status aarbf_set_transfer_functions_rgba8(aarbf_ctx *ctx, const uint8_t *colormap, int nc,
+                                                const uint8_t *radiusmap, int nr,
+                                                const uint8_t *densitymap, int nd);
+/* fp32 tables (native mode): colormap RGBA x nc (rgb linear), radiusmap x nr, densitymap x nd. */
+aarbf_status aarbf_set_transfer_functions_f32(aarbf_ctx *ctx, const float *colormap, int nc,
+                                              const float *radiusmap, int nr,
+                                              const float *densitymap, int nd);
+/* Gradient marks -> 64-entry RGBA8 texture as hostCode.cpp:528-542 (gamma 1/2.2 on rgb when
+ * gamma != 0) and :544-572 (grey maps). marks: npos positions + npos RGBA colours. */
+aarbf_status aarbf_marks_to_rgba8(const float *pos, const float *rgba, int nmarks, int gamma,
+                                  uint8_t *out, int ntexels);
+
+/* ---- acceleration structure -------------------------------------------------------------- */
+
+/* Hilbert keys, device radix sort, attribute normalisation, per-particle shading prepass,
+ * leaf bounds (GenRBFBounds, deviceCodeBounds.hlsl:29-82), Karras LBVH and refit. Replaces
+ * GenRBFBounds + gprtAccelBuild (hostCode.cpp:770-789). Synchronises `stream` once. */
+aarbf_status aarbf_build(aarbf_ctx *ctx, float rbf_radius, uint32_t particles_per_leaf, void *stream);
+/* New radius / transfer functions, same particles: prepass + leaf bounds + refit
+ * (replaces gprtAccelUpdate, hostCode.cpp:791-794). */
+aarbf_status aarbf_refit(aarbf_ctx *ctx, float rbf_radius, void *stream);
+
+/* ---- rendering --------------------------------------------------------------------------- */
+
+/* ParticleRBFRayGen (deviceCodeRBF.hlsl:206-336) with the intersection/any-hit programs
+ * (:338-389) fused in; replaces gprtRayGenLaunch2D(ParticleRBFRayGen) (hostCode.cpp:813).
+ * accum is read-modify-written (running mean over accum_id), image receives the frame. */
+aarbf_status aarbf_render(aarbf_ctx *ctx, const aarbf_params *p, int width, int height,
+                          float *accum, float *image, void *stream);
+/* aarbf_render plus accounting (no counterpart in the reference; for roofline figures):
+ * counts[0] = particles whose sphere meets a traversed ray segment (primary [start, termination]
+ * and shadow), counts[1] = BVH nodes those segment queries visit. Synchronises `stream`. */
+aarbf_status aarbf_render_count(aarbf_ctx *ctx, const aarbf_params *p, int width, int height,
+                                float *accum, float *image, uint64_t *counts, void *stream);
+/* ParticleSplatRayGen (deviceCodeSplat.hlsl:58-193); writes image only. */
+aarbf_status aarbf_render_splat(aarbf_ctx *ctx, const aarbf_params *p, int width, int height,
+                                float *image, void *stream);
+/* CompositeGui TAA resolve (deviceCodeCommon.hlsl:67-115). Writes taa unless disable; bgra
+ * (optional) receives the BGRA8 frame. The reference's taa->taaPrev copy
+ * (hostCode.cpp:829-830) is a pointer swap for the caller. ctx may be NULL. */
+aarbf_status aarbf_taa_resolve(aarbf_ctx *ctx, const float *image, const float *taa_prev,
+                               float *taa, uint32_t *bgra, int width, int height, int disable,
+                               void *stream);
+/* Device buffers owned by the context (GPRT device buffers, hostCode.cpp:314-322). */
+aarbf_status aarbf_get_framebuffers(aarbf_ctx *ctx, int width, int height, float **accum,
+                                    float **image);
+
+/* Device buffers for callers without their own CUDA runtime: gprtDeviceBufferCreate /
+ * gprtBufferDestroy (hostCode.cpp:314-325, :834-836). aarbf_memcpy copies between any mix of
+ * host and device pointers on `stream` (replaces gprtBufferMap + memcpy, hostCode.cpp:759-763). */
+aarbf_status aarbf_device_alloc(aarbf_ctx *ctx, size_t bytes, void **ptr);
+aarbf_status aarbf_device_free(aarbf_ctx *ctx, void *ptr);
+aarbf_status aarbf_memcpy(aarbf_ctx *ctx, void *dst, const void *src, size_t bytes, void *stream);
+aarbf_status aarbf_memset(aarbf_ctx *ctx, void *dst, int value, size_t bytes, void *stream);
+
+/* Blue-noise atlas for the marching mode: RGBA8, 8 x 16 tiles of 256 x 256 (stbn.png layout,
+ * hostCode.cpp:337-352). NULL selects a generated substitute (aarbf_generate_noise_atlas). */
+aarbf_status aarbf_set_noise_atlas(aarbf_ctx *ctx, const uint8_t *rgba8, int width, int height);
+aarbf_status aarbf_generate_noise_atlas(uint8_t *rgba8_out, int width, int height);
+
+/* ---- host helpers ------------------------------------------------------------------------ */
+
+/* Camera basis of hostCode.cpp:669-676 (cos_fovy is the reference's --camera 10th value). */
+aarbf_status aarbf_camera(const float *look_from, const float *look_at, const float *look_up,
+                          float cos_fovy, int width, int height, float *pos, float *dir00,
+                          float *du, float *dv);
+
+/* importParticles (importParticles.h:8-31): header text file of timestep names, each
+ * `path + "_" + name` holding u64 count + count float4. Unlike the reference every read is
+ * checked. */
+typedef struct aarbf_series aarbf_series;
+aarbf_status aarbf_series_load(const char *path, aarbf_series **out);
+aarbf_status aarbf_series_num_frames(const aarbf_series *s, uint64_t *frames);
+aarbf_status aarbf_series_frame(const aarbf_series *s, uint64_t frame, const float **xyzw,
+                                uint64_t *n);
+aarbf_status aarbf_series_free(aarbf_series *s);
+/* writer of the same format (names are "0", "1", ...) */
+aarbf_status aarbf_series_save(const char *path, const float *const *frames, const uint64_t *counts,
+                               uint64_t nframes);
+
+/* ---- debug getters (bit-exact tests) ------------------------------------------------------ */
+
+aarbf_status aarbf_get_num_particles(const aarbf_ctx *ctx, uint64_t *n, uint32_t *num_leaves);
+/* Hilbert keys (in sorted order) and the sort permutation (sorted -> input index) */
+aarbf_status aarbf_get_hilbert_keys(aarbf_ctx *ctx, uint64_t *keys, uint32_t *perm);
+/* sorted, normalised particles (float4 x n) */
+aarbf_status aarbf_get_sorted_particles(aarbf_ctx *ctx, float *xyzw);
+/* prepass records: rec0 = (x,y,z,r_eval) x n, w4 = (a^3, pow(rgb,2.2) a^3) x n, rgeom x n */
+aarbf_status aarbf_get_prepass(aarbf_ctx *ctx, float *rec0, float *w4, float *rgeom);
+/* BVH: child codes (bit31 = leaf) of the L-1 internal nodes, their boxes (6 floats each:
+ * lo xyz, hi xyz), leaf boxes (6 x L) and the root box (6) */
+aarbf_status aarbf_get_bvh(aarbf_ctx *ctx, uint32_t *left, uint32_t *right, float *node_box,
+                           float *leaf_box, float *root_box);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AARBF_H */

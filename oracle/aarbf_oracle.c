@@ -1,0 +1,1165 @@
+/*
+ * aarbf_oracle.c -- TEST INFRASTRUCTURE ONLY (see aarbf_oracle.h).
+ *
+ * A plain-C restatement of the reference's particle-volume path, written from the
+ * reference's semantics. Each function cites the reference file:line it restates.
+ * Compiled with -ffp-contract=off: every float operation below is one IEEE
+ * round-to-nearest operation, fmaf() is written out where a fused step is meant.
+ *
+ * Parity model fixed here (the reference leaves these to the un-vendored GPRT runtime
+ * or to hardware; each choice is documented in DESIGN.md):
+ *   - exp/log/pow: Cody-Waite reduction + Taylor / atanh series (orc_expf/orc_logf);
+ *   - textures: linear filter at texel centres, clamp-to-edge, sRGB decode of R,G,B;
+ *   - any-hit accumulation: exact fixed-point sums (2^-40 units), order independent;
+ *   - sort ties: (key, x, y, z, w, original index);
+ *   - splat: the 15 kept samples of a slab are the 15 smallest (t, index).
+ */
+#include "aarbf_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define ORC_MAX_DEPTH 10000 /* sharedCode.h:27 */
+#define ORC_FIX_SCALE 0x1p40f
+#define ORC_FIX_INV 0x1p-40f
+#define ORC_LEAF_BIT 0x80000000u
+
+static int g_threads = 0;
+void orc_set_threads(int n) { g_threads = n; }
+
+/* ------------------------------------------------------------------------------------------ */
+/* deterministic math                                                                          */
+/* ------------------------------------------------------------------------------------------ */
+
+/* ln 2 split so that k*LN2_HI is exact for |k| < 2^8 (16 significant bits in LN2_HI). */
+static const float LN2_HI = 0x1.62e4p-1f;
+static const float LN2_LO = 0x1.7f7d1cp-20f;
+static const float INV_LN2 = 0x1.715476p+0f;
+static const float SQRT2F = 0x1.6a09e6p+0f;
+
+static inline uint32_t f2u(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+static inline float u2f(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+static inline float pow2i(int k) { return u2f((uint32_t)(k + 127) << 23); } /* -126 <= k <= 127 */
+
+/* natural log: x = m * 2^e with m in [sqrt(1/2), sqrt(2)); log m = 2 atanh(s), s=(m-1)/(m+1),
+ * atanh by its Taylor series through s^9. */
+float orc_logf(float x) {
+  if (x != x || x < 0.0f) return NAN;
+  if (x == 0.0f) return -INFINITY;
+  if (x == INFINITY) return INFINITY;
+  int e = 0;
+  uint32_t b = f2u(x);
+  if (b < 0x00800000u) { x = x * 0x1p23f; b = f2u(x); e = -23; }
+  e += (int)(b >> 23) - 127;
+  float m = u2f((b & 0x007fffffu) | 0x3f800000u);
+  if (m > SQRT2F) { m = m * 0.5f; e += 1; }
+  float s = (m - 1.0f) / (m + 1.0f);
+  float z = s * s;
+  float p = 0x1.c71c72p-3f;          /* 2/9 */
+  p = fmaf(p, z, 0x1.24924ap-2f);   /* 2/7 */
+  p = fmaf(p, z, 0x1.99999ap-2f);   /* 2/5 */
+  p = fmaf(p, z, 0x1.555556p-1f);   /* 2/3 */
+  p = fmaf(p, z, 2.0f);
+  float lm = s * p;
+  float ef = (float)e;
+  return fmaf(ef, LN2_HI, fmaf(ef, LN2_LO, lm));
+}
+
+/* exp: k = rint(x/ln2), r = x - k ln2 (two fused steps), Taylor series through r^7,
+ * scaled by 2^k in two exact power-of-two multiplies (one rounding for subnormals). */
+float orc_expf(float x) {
+  if (x != x) return x;
+  if (x > 88.72284f) return INFINITY;
+  if (x < -103.972084f) return 0.0f;
+  float kf = rintf(x * INV_LN2);
+  float r = fmaf(-kf, LN2_HI, x);
+  r = fmaf(-kf, LN2_LO, r);
+  float p = 0x1.a01a02p-13f;        /* 1/5040 */
+  p = fmaf(p, r, 0x1.6c16c2p-10f);  /* 1/720 */
+  p = fmaf(p, r, 0x1.111112p-7f);   /* 1/120 */
+  p = fmaf(p, r, 0x1.555556p-5f);   /* 1/24 */
+  p = fmaf(p, r, 0x1.555556p-3f);   /* 1/6 */
+  p = fmaf(p, r, 0.5f);
+  p = fmaf(p, r, 1.0f);
+  p = fmaf(p, r, 1.0f);
+  int k = (int)kf;
+  int k1 = k / 2;
+  int k2 = k - k1;
+  return (p * pow2i(k1)) * pow2i(k2);
+}
+
+/* pow for x >= 0 as used by the shaders (colour gamma 2.2 and 1/2.2) */
+float orc_powf(float x, float y) {
+  if (x != x || y != y) return NAN;
+  if (x == 0.0f) return (y > 0.0f) ? 0.0f : (y == 0.0f ? 1.0f : INFINITY);
+  if (x < 0.0f) return NAN;
+  return orc_expf(y * orc_logf(x));
+}
+
+static inline float orc_minf(float a, float b) { return fminf(a, b); }
+static inline float orc_maxf(float a, float b) { return fmaxf(a, b); }
+
+/* ------------------------------------------------------------------------------------------ */
+/* Hilbert curve: restates hilbert.h hilbert_c2i (181-225) and hilbert_i2c (124-166),          */
+/* with the bit transpose (37-88) written as an explicit bit loop.                             */
+/* ------------------------------------------------------------------------------------------ */
+
+static inline uint64_t ones64(unsigned k) { return k >= 64 ? ~0ull : ((1ull << k) - 1ull); }
+
+static inline uint64_t rot_right(uint64_t v, unsigned n, unsigned w) {
+  return ((v >> n) | (v << (w - n))) & ones64(w);
+}
+static inline uint64_t rot_left(uint64_t v, unsigned n, unsigned w) {
+  return ((v << n) | (v >> (w - n))) & ones64(w);
+}
+
+/* rotation bookkeeping of hilbert.h:16-24: advance by 1 + index of the lowest set bit of the
+ * digit when that bit lies below the top axis, modulo nDims */
+static inline unsigned next_rotation(unsigned rotation, unsigned nDims, uint64_t digit) {
+  uint64_t low = digit & (~digit + 1ull) & (ones64(nDims) >> 1);
+  while (low) { low >>= 1; ++rotation; }
+  ++rotation;
+  if (rotation >= nDims) rotation -= nDims;
+  return rotation;
+}
+
+uint64_t orc_hilbert_c2i(unsigned nDims, unsigned nBits, const uint64_t *coord) {
+  if (nDims <= 1) return coord[0];
+  const unsigned total = nDims * nBits;
+  /* OR-packing: field d at bits [d*nBits, (d+1)*nBits); a coordinate equal to 2^nBits spills
+   * its top bit into field d+1 exactly as the reference packing does (hilbert.h:189-193) */
+  uint64_t packed = 0;
+  for (int d = (int)nDims - 1; d >= 0; --d) packed = (packed << nBits) | coord[d];
+  uint64_t index;
+  if (nBits > 1) {
+    uint64_t inter = 0;
+    for (unsigned d = 0; d < nDims; ++d) {
+      uint64_t field = (d * nBits < 64) ? ((packed >> (d * nBits)) & ones64(nBits)) : 0;
+      for (unsigned b = 0; b < nBits; ++b)
+        inter |= ((field >> b) & 1ull) << (b * nDims + d);
+    }
+    inter ^= inter >> nDims;
+    index = 0;
+    unsigned rotation = 0;
+    uint64_t flip = 0;
+    for (int b = (int)total - (int)nDims; b >= 0; b -= (int)nDims) {
+      uint64_t digit = (inter >> b) & ones64(nDims);
+      digit = rot_right(flip ^ digit, rotation, nDims);
+      index = (index << nDims) | digit;
+      flip = 1ull << rotation;
+      rotation = next_rotation(rotation, nDims, digit);
+    }
+    index ^= (ones64(total) / ones64(nDims)) >> 1;
+  } else {
+    index = packed;
+  }
+  for (unsigned d = 1; d < total; d *= 2) index ^= index >> d;
+  return index;
+}
+
+void orc_hilbert_i2c(unsigned nDims, unsigned nBits, uint64_t index, uint64_t *coord) {
+  if (nDims <= 1) { coord[0] = index; return; }
+  const unsigned total = nDims * nBits;
+  uint64_t coords;
+  if (nBits > 1) {
+    const uint64_t nth = ones64(total) / ones64(nDims);
+    index ^= (index ^ nth) >> 1;
+    uint64_t inter = 0;
+    unsigned rotation = 0;
+    uint64_t flip = 0;
+    for (int b = (int)total - (int)nDims; b >= 0; b -= (int)nDims) {
+      uint64_t digit = (index >> b) & ones64(nDims);
+      inter = (inter << nDims) | (rot_left(digit, rotation, nDims) ^ flip);
+      flip = 1ull << rotation;
+      rotation = next_rotation(rotation, nDims, digit);
+    }
+    for (unsigned b = nDims; b < total; b *= 2) inter ^= inter >> b;
+    coords = 0;
+    for (unsigned d = 0; d < nDims; ++d)
+      for (unsigned b = 0; b < nBits; ++b)
+        coords |= ((inter >> (b * nDims + d)) & 1ull) << (d * nBits + b);
+  } else {
+    coords = index ^ (index >> 1);
+  }
+  for (unsigned d = 0; d < nDims; ++d) {
+    coord[d] = coords & ones64(nBits);
+    coords >>= nBits;
+  }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* RNG: rng.h:24-70                                                                            */
+/* ------------------------------------------------------------------------------------------ */
+
+static inline uint32_t rotl32(uint32_t v, unsigned r) { return (v << r) | (v >> (32u - r)); }
+
+uint32_t orc_murmur_mix(uint32_t hash, uint32_t k) {
+  k *= 0xcc9e2d51u;
+  k = rotl32(k, 15);
+  k *= 0x1b873593u;
+  hash ^= k;
+  return rotl32(hash, 13) * 5u + 0xe6546b64u;
+}
+
+uint32_t orc_murmur_finalize(uint32_t h) {
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+
+uint32_t orc_get_rng(int frame_id, uint32_t px, uint32_t py, uint32_t dimx) {
+  uint32_t s = orc_murmur_mix(0u, px + py * dimx);
+  s = orc_murmur_mix(s, (uint32_t)frame_id);
+  return orc_murmur_finalize(s);
+}
+
+uint32_t orc_lcg_next(uint32_t *state) {
+  *state = *state * 1664525u + 1013904223u;
+  return *state;
+}
+
+/* ldexp((float)u, -32): the u32 -> float conversion rounds, the scaling is exact */
+float orc_lcg_randomf(uint32_t *state) { return (float)orc_lcg_next(state) * 0x1p-32f; }
+
+/* ------------------------------------------------------------------------------------------ */
+/* host preprocessing: hostCode.cpp:183-250                                                    */
+/* ------------------------------------------------------------------------------------------ */
+
+void orc_domain_init(float *dom) {
+  /* hostCode.cpp:183 starts from +-1e38; attribute range from +-1e20 (:227-228) */
+  dom[0] = dom[1] = dom[2] = 1e38f;
+  dom[3] = dom[4] = dom[5] = -1e38f;
+  dom[6] = 1e20f;
+  dom[7] = -1e20f;
+}
+
+void orc_domain_accumulate(const float *p, uint64_t n, float *dom) {
+  for (uint64_t i = 0; i < n; ++i) {
+    for (int a = 0; a < 3; ++a) {
+      dom[a] = orc_minf(dom[a], p[4 * i + a]);
+      dom[3 + a] = orc_maxf(dom[3 + a], p[4 * i + a]);
+    }
+    dom[6] = orc_minf(dom[6], p[4 * i + 3]);
+    dom[7] = orc_maxf(dom[7], p[4 * i + 3]);
+  }
+}
+
+/* quantise to 16 bits per axis, (p-min)/(max-min)*65536 truncated (hostCode.cpp:200-206).
+ * A degenerate axis (max == min) and coordinates outside the domain are clamped to [0, 65536]
+ * (the reference leaves both undefined). */
+static inline uint64_t quantise16(float v, float lo, float hi) {
+  float t = (v - lo) / (hi - lo);
+  t = t * 65536.0f;
+  if (!(t >= 0.0f)) return 0;
+  if (t >= 65536.0f) return 65536;
+  return (uint64_t)t;
+}
+
+void orc_hilbert_keys(const float *p, uint64_t n, const float *dom, uint64_t *keys) {
+  for (uint64_t i = 0; i < n; ++i) {
+    uint64_t c[3];
+    for (int a = 0; a < 3; ++a) c[a] = quantise16(p[4 * i + a], dom[a], dom[3 + a]);
+    keys[i] = orc_hilbert_c2i(3, 16, c);
+  }
+}
+
+/* total order used for the Hilbert sort: key, then x, y, z, w compared as floats, then index */
+static const uint64_t *g_sort_keys;
+static const float *g_sort_p;
+static int cmp_perm(const void *a, const void *b) {
+  uint32_t i = *(const uint32_t *)a, j = *(const uint32_t *)b;
+  if (g_sort_keys[i] != g_sort_keys[j]) return g_sort_keys[i] < g_sort_keys[j] ? -1 : 1;
+  for (int c = 0; c < 4; ++c) {
+    float x = g_sort_p[4 * (uint64_t)i + c], y = g_sort_p[4 * (uint64_t)j + c];
+    if (x < y) return -1;
+    if (y < x) return 1;
+  }
+  return (i < j) ? -1 : (i > j ? 1 : 0);
+}
+
+void orc_sort_perm(const uint64_t *keys, const float *p, uint64_t n, uint32_t *perm) {
+  for (uint64_t i = 0; i < n; ++i) perm[i] = (uint32_t)i;
+  g_sort_keys = keys;
+  g_sort_p = p;
+  qsort(perm, (size_t)n, sizeof(uint32_t), cmp_perm);
+}
+
+void orc_gather_normalize(const float *p, const float *radii, const uint32_t *perm, uint64_t n,
+                          float amin, float amax, float *out, float *out_r) {
+  for (uint64_t i = 0; i < n; ++i) {
+    uint64_t s = perm[i];
+    out[4 * i + 0] = p[4 * s + 0];
+    out[4 * i + 1] = p[4 * s + 1];
+    out[4 * i + 2] = p[4 * s + 2];
+    float w = p[4 * s + 3];
+    if (amax > amin) w = (w - amin) / (amax - amin); /* hostCode.cpp:243-250 */
+    out[4 * i + 3] = w;
+    if (radii && out_r) out_r[i] = radii[s];
+  }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* transfer functions                                                                          */
+/* ------------------------------------------------------------------------------------------ */
+
+/* hostCode.cpp:524-526 */
+uint8_t orc_make_8bit(float f) {
+  int v = (int)(f * 256.0f);
+  if (v < 0) v = 0;
+  if (v > 255) v = 255;
+  return (uint8_t)v;
+}
+
+static float srgb_decode8(uint8_t v) {
+  double c = (double)v / 255.0;
+  double l = (c <= 0.04045) ? c / 12.92 : pow((c + 0.055) / 1.055, 2.4);
+  return (float)l;
+}
+
+/* R8G8B8A8_SRGB textures (hostCode.cpp:355-365): R,G,B decoded, alpha linear */
+void orc_decode_rgba8(const uint8_t *t, int n, int srgb, float *out) {
+  for (int i = 0; i < n; ++i) {
+    for (int c = 0; c < 3; ++c)
+      out[4 * i + c] = srgb ? srgb_decode8(t[4 * i + c]) : (float)((double)t[4 * i + c] / 255.0);
+    out[4 * i + 3] = (float)((double)t[4 * i + 3] / 255.0);
+  }
+}
+
+/* SampleGrad with zero gradients: linear filter between texel centres, clamp to edge */
+float orc_tex_sample(const float *tex, int n, int stride, int channel, float u) {
+  float f = u * (float)n - 0.5f;
+  if (!(f > -1.0f)) f = -1.0f;
+  if (f > (float)n) f = (float)n;
+  float fl = floorf(f);
+  float a = f - fl;
+  int i0 = (int)fl;
+  int i1 = i0 + 1;
+  if (i0 < 0) i0 = 0;
+  if (i0 > n - 1) i0 = n - 1;
+  if (i1 < 0) i1 = 0;
+  if (i1 > n - 1) i1 = n - 1;
+  float v0 = tex[i0 * stride + channel];
+  float v1 = tex[i1 * stride + channel];
+  return v0 + a * (v1 - v0);
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* camera (hostCode.cpp:669-676) and light (sharedCode.h:127-132)                               */
+/* ------------------------------------------------------------------------------------------ */
+
+static void v3_normalize(const float *a, float *o) {
+  float len = sqrtf((a[0] * a[0] + a[1] * a[1]) + a[2] * a[2]);
+  o[0] = a[0] / len;
+  o[1] = a[1] / len;
+  o[2] = a[2] / len;
+}
+static void v3_cross(const float *a, const float *b, float *o) {
+  float x = a[1] * b[2] - a[2] * b[1];
+  float y = a[2] * b[0] - a[0] * b[2];
+  float z = a[0] * b[1] - a[1] * b[0];
+  o[0] = x; o[1] = y; o[2] = z;
+}
+
+void orc_camera(const float *from, const float *at, const float *up, float cos_fovy, int width,
+                int height, float *pos, float *d00, float *du, float *dv) {
+  float diff[3] = {at[0] - from[0], at[1] - from[1], at[2] - from[2]};
+  float dir[3], c[3], n[3];
+  v3_normalize(diff, dir);
+  float aspect = (float)width / (float)height;
+  v3_cross(dir, up, c);
+  v3_normalize(c, n);
+  float su = cos_fovy * aspect;
+  float ddu[3] = {su * n[0], su * n[1], su * n[2]};
+  v3_cross(ddu, dir, c);
+  v3_normalize(c, n);
+  float ddv[3] = {cos_fovy * n[0], cos_fovy * n[1], cos_fovy * n[2]};
+  for (int a = 0; a < 3; ++a) {
+    float d = dir[a] - 0.5f * ddu[a];
+    d = d - 0.5f * ddv[a];
+    pos[a] = from[a];
+    d00[a] = d;
+    du[a] = ddu[a];
+    dv[a] = ddv[a];
+  }
+}
+
+void orc_light_dir(float az, float el, float *dir) {
+  float a = el * 3.14f - 0.5f * 3.14f;
+  float b = (az * 2.0f) * 3.14f;
+  float s = sinf(a);
+  dir[0] = s * cosf(b);
+  dir[1] = s * sinf(b);
+  dir[2] = cosf(a);
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* scene: per-particle prepass, leaf bounds (deviceCodeBounds.hlsl:29-82), Karras LBVH, refit  */
+/* ------------------------------------------------------------------------------------------ */
+
+struct orc_scene {
+  uint64_t n;
+  uint32_t ppl, nleaves;
+  float rbf_radius;
+  float *xyzw;     /* 4n sorted particles (attribute normalised) */
+  float *rec0;     /* 4n: x, y, z, r_eval (0 when the particle can never be hit) */
+  float *w4;       /* 4n: alpha^3, pow(r,2.2) a^3, pow(g,2.2) a^3, pow(b,2.2) a^3 */
+  float *rgeom;    /* n: bounds radius, -1 when radiusmap == 0 (skipped by the bounds program) */
+  uint64_t *leaf_key;
+  float *leaf_box; /* 6 per leaf */
+  uint32_t *left, *right;
+  float *node_box; /* 6 per internal node */
+  float root_box[6];
+  uint32_t root;   /* child code of the root */
+  /* transfer functions for rendering */
+  float *color; int nc;
+  float *density; int nd;
+};
+
+static float *dupf(const float *src, size_t cnt) {
+  float *d = (float *)malloc(cnt * sizeof(float));
+  memcpy(d, src, cnt * sizeof(float));
+  return d;
+}
+
+/* deviceCodeRBF.hlsl:349-351 (radius), :366-376 (colour weights), deviceCodeBounds.hlsl:59-65 */
+static void prepass(orc_scene *s, const float *radii, const orc_tf_desc *tf) {
+  for (uint64_t i = 0; i < s->n; ++i) {
+    const float *p = s->xyzw + 4 * i;
+    float w = p[3];
+    float rp = orc_tex_sample(tf->radius, tf->nr, 1, 0, w);
+    float base = radii ? radii[i] : s->rbf_radius;
+    float r = base * rp;
+    float col[4];
+    for (int c = 0; c < 4; ++c) col[c] = orc_tex_sample(tf->color, tf->nc, 4, c, w);
+    s->rgeom[i] = (rp == 0.0f) ? -1.0f : r;
+    s->rec0[4 * i + 0] = p[0];
+    s->rec0[4 * i + 1] = p[1];
+    s->rec0[4 * i + 2] = p[2];
+    float a = col[3];
+    if (a == 0.0f) {
+      s->rec0[4 * i + 3] = 0.0f;
+      s->w4[4 * i + 0] = s->w4[4 * i + 1] = s->w4[4 * i + 2] = s->w4[4 * i + 3] = 0.0f;
+    } else {
+      float a3 = (a * a) * a;
+      s->rec0[4 * i + 3] = r;
+      s->w4[4 * i + 0] = a3;
+      for (int c = 0; c < 3; ++c) s->w4[4 * i + 1 + c] = orc_powf(col[c], 2.2f) * a3;
+    }
+  }
+}
+
+static void leaf_bounds(orc_scene *s) {
+  for (uint32_t l = 0; l < s->nleaves; ++l) {
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t k = 0; k < s->ppl; ++k) {
+      uint64_t i = (uint64_t)l * s->ppl + k;
+      if (i >= s->n) break;
+      float r = s->rgeom[i];
+      if (r < 0.0f) continue; /* radiusPercent == 0 */
+      for (int a = 0; a < 3; ++a) {
+        float c = s->rec0[4 * i + a];
+        lo[a] = orc_minf(lo[a], c - r);
+        hi[a] = orc_maxf(hi[a], c + r);
+      }
+    }
+    int empty = (lo[0] > hi[0]) || (lo[1] > hi[1]) || (lo[2] > hi[2]);
+    for (int a = 0; a < 3; ++a) {
+      s->leaf_box[6 * l + a] = empty ? NAN : lo[a];
+      s->leaf_box[6 * l + 3 + a] = empty ? NAN : hi[a];
+    }
+  }
+}
+
+/* Karras (HPG 2012) radix tree over leaf keys; equal keys are ordered by leaf index */
+static int delta(const uint64_t *k, int64_t L, int64_t i, int64_t j) {
+  if (j < 0 || j >= L) return -1;
+  uint64_t x = k[i] ^ k[j];
+  if (x == 0) return 64 + __builtin_clz((uint32_t)(i ^ j));
+  return __builtin_clzll(x);
+}
+
+static void karras(orc_scene *s) {
+  const int64_t L = s->nleaves;
+  const uint64_t *k = s->leaf_key;
+  for (int64_t i = 0; i < L - 1; ++i) {
+    int d = (delta(k, L, i, i + 1) - delta(k, L, i, i - 1)) >= 0 ? 1 : -1;
+    int dmin = delta(k, L, i, i - d);
+    int64_t lmax = 2;
+    while (delta(k, L, i, i + lmax * d) > dmin) lmax *= 2;
+    int64_t l = 0;
+    for (int64_t t = lmax / 2; t >= 1; t /= 2)
+      if (delta(k, L, i, i + (l + t) * d) > dmin) l += t;
+    int64_t j = i + l * d;
+    int dnode = delta(k, L, i, j);
+    int64_t sp = 0, step = l;
+    do {
+      step = (step + 1) >> 1;
+      if (delta(k, L, i, i + (sp + step) * d) > dnode) sp += step;
+    } while (step > 1);
+    int64_t g = i + sp * d + (d < 0 ? -1 : 0);
+    int64_t lo = i < j ? i : j, hi = i < j ? j : i;
+    s->left[i] = (lo == g) ? ((uint32_t)g | ORC_LEAF_BIT) : (uint32_t)g;
+    s->right[i] = (hi == g + 1) ? ((uint32_t)(g + 1) | ORC_LEAF_BIT) : (uint32_t)(g + 1);
+  }
+}
+
+static const float *child_box(const orc_scene *s, uint32_t c) {
+  return (c & ORC_LEAF_BIT) ? s->leaf_box + 6 * (c & ~ORC_LEAF_BIT) : s->node_box + 6 * c;
+}
+
+static void refit_node(orc_scene *s, uint32_t node) {
+  /* post-order over the internal nodes; explicit stack */
+  uint32_t *stack = (uint32_t *)malloc(sizeof(uint32_t) * 2 * (s->nleaves + 1));
+  uint8_t *state = (uint8_t *)calloc(s->nleaves, 1);
+  int sp = 0;
+  stack[sp++] = node;
+  while (sp) {
+    uint32_t nd = stack[sp - 1];
+    if (!state[nd]) {
+      state[nd] = 1;
+      if (!(s->left[nd] & ORC_LEAF_BIT)) stack[sp++] = s->left[nd];
+      if (!(s->right[nd] & ORC_LEAF_BIT)) stack[sp++] = s->right[nd];
+      continue;
+    }
+    --sp;
+    const float *a = child_box(s, s->left[nd]);
+    const float *b = child_box(s, s->right[nd]);
+    for (int c = 0; c < 3; ++c) {
+      s->node_box[6 * nd + c] = orc_minf(a[c], b[c]);
+      s->node_box[6 * nd + 3 + c] = orc_maxf(a[3 + c], b[3 + c]);
+    }
+  }
+  free(stack);
+  free(state);
+}
+
+orc_scene *orc_scene_create(const float *xyzw, const float *radii, const uint64_t *keys, uint64_t n,
+                            uint32_t ppl, float rbf_radius, const orc_tf_desc *tf) {
+  orc_scene *s = (orc_scene *)calloc(1, sizeof(orc_scene));
+  s->n = n;
+  s->ppl = ppl ? ppl : 1;
+  s->rbf_radius = rbf_radius;
+  s->nleaves = (uint32_t)((n + s->ppl - 1) / s->ppl);
+  size_t nn = n ? n : 1, nl = s->nleaves ? s->nleaves : 1;
+  s->xyzw = dupf(xyzw ? xyzw : (const float[4]){0, 0, 0, 0}, n ? 4 * n : 4);
+  s->rec0 = (float *)calloc(4 * nn, sizeof(float));
+  s->w4 = (float *)calloc(4 * nn, sizeof(float));
+  s->rgeom = (float *)calloc(nn, sizeof(float));
+  s->leaf_key = (uint64_t *)calloc(nl, sizeof(uint64_t));
+  s->leaf_box = (float *)calloc(6 * nl, sizeof(float));
+  s->left = (uint32_t *)calloc(nl, sizeof(uint32_t));
+  s->right = (uint32_t *)calloc(nl, sizeof(uint32_t));
+  s->node_box = (float *)calloc(6 * nl, sizeof(float));
+  s->color = dupf(tf->color, 4 * (size_t)tf->nc);
+  s->nc = tf->nc;
+  s->density = dupf(tf->density, (size_t)tf->nd);
+  s->nd = tf->nd;
+  prepass(s, radii, tf);
+  for (uint32_t l = 0; l < s->nleaves; ++l) s->leaf_key[l] = keys[(uint64_t)l * s->ppl];
+  leaf_bounds(s);
+  if (s->nleaves == 0) {
+    for (int a = 0; a < 6; ++a) s->root_box[a] = NAN;
+    s->root = ORC_LEAF_BIT; /* unused */
+  } else if (s->nleaves == 1) {
+    s->root = 0 | ORC_LEAF_BIT;
+    memcpy(s->root_box, s->leaf_box, 6 * sizeof(float));
+  } else {
+    karras(s);
+    refit_node(s, 0);
+    s->root = 0;
+    memcpy(s->root_box, s->node_box, 6 * sizeof(float));
+  }
+  return s;
+}
+
+void orc_scene_destroy(orc_scene *s) {
+  if (!s) return;
+  free(s->xyzw); free(s->rec0); free(s->w4); free(s->rgeom);
+  free(s->leaf_key); free(s->leaf_box); free(s->left); free(s->right); free(s->node_box);
+  free(s->color); free(s->density);
+  free(s);
+}
+
+uint32_t orc_scene_num_leaves(const orc_scene *s) { return s->nleaves; }
+
+void orc_scene_get_bvh(const orc_scene *s, uint32_t *left, uint32_t *right, float *node_box,
+                       float *leaf_box, float *root_box) {
+  uint32_t ni = s->nleaves > 0 ? s->nleaves - 1 : 0;
+  if (left) memcpy(left, s->left, ni * sizeof(uint32_t));
+  if (right) memcpy(right, s->right, ni * sizeof(uint32_t));
+  if (node_box) memcpy(node_box, s->node_box, 6 * (size_t)ni * sizeof(float));
+  if (leaf_box) memcpy(leaf_box, s->leaf_box, 6 * (size_t)s->nleaves * sizeof(float));
+  if (root_box) memcpy(root_box, s->root_box, 6 * sizeof(float));
+}
+
+void orc_scene_get_prepass(const orc_scene *s, float *rec0, float *w4, float *rgeom) {
+  if (rec0) memcpy(rec0, s->rec0, 4 * s->n * sizeof(float));
+  if (w4) memcpy(w4, s->w4, 4 * s->n * sizeof(float));
+  if (rgeom) memcpy(rgeom, s->rgeom, s->n * sizeof(float));
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* point query = ParticleRBFIntersection + ParticleRBFAnyHit (deviceCodeRBF.hlsl:338-389)      */
+/* ------------------------------------------------------------------------------------------ */
+
+static inline int64_t fix40(float v) { return llrintf(v * ORC_FIX_SCALE); }
+
+static inline void eval_particle(const orc_scene *s, uint64_t i, const float *x, int *count,
+                                 int64_t *acc) {
+  const float *r = s->rec0 + 4 * i;
+  float dx = r[0] - x[0], dy = r[1] - x[1], dz = r[2] - x[2];
+  float dist = sqrtf((dx * dx + dy * dy) + dz * dz);
+  if (!(dist < r[3])) return;
+  /* evaluate_rbf, sharedCode.h:137-140, sigma = 3 */
+  float q = (dist * 3.0f) / r[3];
+  float rho = orc_expf(-0.5f * (q * q));
+  const float *w = s->w4 + 4 * i;
+  *count += 1;
+  acc[0] += fix40(rho * w[0]);
+  acc[1] += fix40(rho * w[1]);
+  acc[2] += fix40(rho * w[2]);
+  acc[3] += fix40(rho * w[3]);
+}
+
+static inline int box_contains(const float *b, const float *x) {
+  return x[0] >= b[0] && x[0] <= b[3] && x[1] >= b[1] && x[1] <= b[4] && x[2] >= b[2] &&
+         x[2] <= b[5];
+}
+
+static void leaf_eval(const orc_scene *s, uint32_t leaf, const float *x, int *count,
+                      int64_t *acc) {
+  for (uint32_t k = 0; k < s->ppl; ++k) {
+    uint64_t i = (uint64_t)leaf * s->ppl + k;
+    if (i >= s->n) break;
+    eval_particle(s, i, x, count, acc);
+  }
+}
+
+int orc_point_query(const orc_scene *s, const float *x, int64_t *acc) {
+  int count = 0;
+  acc[0] = acc[1] = acc[2] = acc[3] = 0;
+  if (s->nleaves == 0 || !box_contains(s->root_box, x)) return 0;
+  if (s->root & ORC_LEAF_BIT) {
+    leaf_eval(s, s->root & ~ORC_LEAF_BIT, x, &count, acc);
+    return count;
+  }
+  uint32_t stack[128];
+  int sp = 0;
+  stack[sp++] = s->root;
+  while (sp) {
+    uint32_t nd = stack[--sp];
+    uint32_t ch[2] = {s->left[nd], s->right[nd]};
+    for (int c = 0; c < 2; ++c) {
+      if (!box_contains(child_box(s, ch[c]), x)) continue;
+      if (ch[c] & ORC_LEAF_BIT) leaf_eval(s, ch[c] & ~ORC_LEAF_BIT, x, &count, acc);
+      else if (sp < 128) stack[sp++] = ch[c];
+      else abort(); /* tree deeper than any 64-bit key prefix allows */
+    }
+  }
+  return count;
+}
+
+int orc_point_query_brute(const orc_scene *s, const float *x, int64_t *acc) {
+  int count = 0;
+  acc[0] = acc[1] = acc[2] = acc[3] = 0;
+  for (uint64_t i = 0; i < s->n; ++i) eval_particle(s, i, x, &count, acc);
+  return count;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* tracker: ParticleTracker (deviceCodeRBF.hlsl:40-204)                                         */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct {
+  float o[3], d[3], tmin, tmax;
+} orc_ray;
+
+typedef struct {
+  int i;
+  float random;
+  uint32_t rng;
+  float albedo[4];
+  float t;
+  float lhs;
+  int shadow;
+  int marching;
+} orc_tracker;
+
+/* sharedCode.h:151-185 */
+static int aabb_intersect(const orc_ray *r, const float *lb, const float *rt, float *tenter,
+                          float *texit) {
+  float fx = 1.0f / r->d[0], fy = 1.0f / r->d[1], fz = 1.0f / r->d[2];
+  float t2 = (rt[0] - r->o[0]) * fx;
+  float t4 = (rt[1] - r->o[1]) * fy;
+  float t6 = (rt[2] - r->o[2]) * fz;
+  float t1 = (lb[0] - r->o[0]) * fx;
+  float t3 = (lb[1] - r->o[1]) * fy;
+  float t5 = (lb[2] - r->o[2]) * fz;
+  float te = orc_maxf(orc_maxf(orc_minf(t1, t2), orc_minf(t3, t4)), orc_minf(t5, t6));
+  float tx = orc_minf(orc_minf(orc_maxf(t1, t2), orc_maxf(t3, t4)), orc_maxf(t5, t6));
+  te = orc_maxf(te, r->tmin);
+  tx = orc_minf(tx, r->tmax);
+  *tenter = te;
+  *texit = tx;
+  int hit = 1;
+  if (tx < 0.0f) hit = 0;
+  if (te >= tx) hit = 0;
+  return hit;
+}
+
+typedef struct {
+  int count;
+  float density; /* D */
+  float c[3];    /* C (not yet divided) */
+} orc_sample;
+
+static void sample_at(const orc_scene *s, const float *x, orc_sample *out) {
+  int64_t acc[4];
+  out->count = orc_point_query(s, x, acc);
+  out->density = (float)acc[0] * ORC_FIX_INV;
+  out->c[0] = (float)acc[1] * ORC_FIX_INV;
+  out->c[1] = (float)acc[2] * ORC_FIX_INV;
+  out->c[2] = (float)acc[3] * ORC_FIX_INV;
+}
+
+/* colour of a sample, deviceCodeRBF.hlsl:184-186 (+:192-194 when not visualising attributes) */
+static void sample_color(const orc_scene *s, const orc_params *p, const orc_sample *smp,
+                         float *rgb) {
+  if (p->flags & ORC_FLAG_VISUALIZE_ATTRIBUTES) {
+    for (int c = 0; c < 3; ++c) rgb[c] = orc_powf(smp->c[c] / smp->density, 1.0f / 2.2f);
+  } else {
+    for (int c = 0; c < 3; ++c) rgb[c] = orc_tex_sample(s->color, s->nc, 4, c, smp->density);
+  }
+}
+
+/* densitymap(D) (:190), or the native linear transform min(D*gain, 1) */
+static float sample_density(const orc_scene *s, const orc_params *p, float D) {
+  if (p->flags & ORC_FLAG_DENSITY_LINEAR) return orc_minf(D * p->density_gain, 1.0f);
+  return orc_tex_sample(s->density, s->nd, 1, 0, D);
+}
+
+/* stochasticTracking, deviceCodeRBF.hlsl:141-203 */
+static void track_delta(const orc_scene *s, const orc_params *p, orc_tracker *tr,
+                        const orc_ray *ray, int from_entry) {
+  if (!from_entry) tr->t = ray->tmin;
+  for (; tr->i < ORC_MAX_DEPTH; ++tr->i) {
+    float u = orc_lcg_randomf(&tr->rng);
+    float step = (orc_logf(1.0f - u) / 1.0f) * p->unit;
+    tr->t = tr->t - step;
+    if (tr->t >= ray->tmax) return;
+    float x[3] = {ray->o[0] + tr->t * ray->d[0], ray->o[1] + tr->t * ray->d[1],
+                  ray->o[2] + tr->t * ray->d[2]};
+    orc_sample smp;
+    sample_at(s, x, &smp);
+    if (smp.count == 0) continue;
+    float density = sample_density(s, p, smp.density);
+    if (orc_lcg_randomf(&tr->rng) < density / 1.0f) {
+      float rgb[3];
+      sample_color(s, p, &smp, rgb);
+      tr->albedo[0] = rgb[0];
+      tr->albedo[1] = rgb[1];
+      tr->albedo[2] = rgb[2];
+      tr->albedo[3] = 1.0f;
+      return;
+    }
+  }
+}
+
+/* stochasticMarching, deviceCodeRBF.hlsl:67-139 */
+static void track_march(const orc_scene *s, const orc_params *p, orc_tracker *tr,
+                        const orc_ray *ray) {
+  float rhs = -orc_logf(1.0f - tr->random * 0.99f);
+  for (; tr->i < ORC_MAX_DEPTH; ++tr->i) {
+    tr->t = tr->t + p->unit;
+    if (tr->t >= ray->tmax) return;
+    float x[3] = {ray->o[0] + tr->t * ray->d[0], ray->o[1] + tr->t * ray->d[1],
+                  ray->o[2] + tr->t * ray->d[2]};
+    orc_sample smp;
+    sample_at(s, x, &smp);
+    if (!(smp.count > 0 && smp.density > 0.0f)) continue;
+    float density = sample_density(s, p, smp.density);
+    tr->lhs = tr->lhs + density;
+    if (tr->lhs > rhs && !tr->shadow) {
+      float rgb[3];
+      sample_color(s, p, &smp, rgb);
+      tr->albedo[0] = rgb[0];
+      tr->albedo[1] = rgb[1];
+      tr->albedo[2] = rgb[2];
+      tr->albedo[3] = 1.0f;
+      return;
+    }
+    if (tr->shadow) {
+      tr->albedo[3] = tr->albedo[3] + (1.0f - orc_expf(-density));
+      if (tr->albedo[3] >= 1.0f) {
+        tr->albedo[3] = 1.0f;
+        return;
+      }
+    }
+  }
+}
+
+static void track(const orc_scene *s, const orc_params *p, orc_tracker *tr, const orc_ray *ray,
+                  int from_entry) {
+  if (tr->marching) track_march(s, p, tr, ray);
+  else track_delta(s, p, tr, ray, from_entry);
+}
+
+/* sharedCode.h:142-150 */
+static void over(const float *a, const float *b, float *res) {
+  float ra = a[3] + b[3] * (1.0f - a[3]);
+  if (ra == 0.0f) {
+    res[0] = a[0]; res[1] = a[1]; res[2] = a[2]; res[3] = a[3];
+    return;
+  }
+  for (int c = 0; c < 3; ++c) res[c] = (a[c] * a[3] + (b[c] * b[3]) * (1.0f - a[3])) / ra;
+  res[3] = ra;
+}
+
+static float noise_at(const orc_params *p, uint32_t frame, uint32_t px, uint32_t py) {
+  /* deviceCodeRBF.hlsl:243-251: 8 x 16 grid of 256x256 tiles, UNORM8 .x */
+  uint32_t gx = frame % 8u, gy = (frame / 8u) % 16u;
+  uint32_t cx = gx * 256u + px % 256u, cy = gy * 256u + py % 256u;
+  if (!p->noise || (int)cx >= p->noise_w || (int)cy >= p->noise_h) return 0.0f;
+  uint8_t v = p->noise[4 * ((size_t)cy * (size_t)p->noise_w + cx)];
+  return (float)v / 255.0f;
+}
+
+/* ParticleRBFRayGen, deviceCodeRBF.hlsl:206-336, one sample; returns colour (pre-accumulation)
+ * and the noise value used for showNoise */
+static void raygen_sample(const orc_scene *s, const orc_params *p, const float *light, uint32_t frame,
+                          int px, int py, int w, int h, float *color, float *noise_out) {
+  uint32_t rng = orc_get_rng((int)frame, (uint32_t)px, (uint32_t)py, (uint32_t)w);
+  float sx = ((float)px + 0.5f + p->jitter_x) / (float)w;
+  float sy = ((float)py + 0.5f + p->jitter_y) / (float)h;
+  float rt[3], lb[3];
+  for (int a = 0; a < 3; ++a) {
+    rt[a] = p->aabb_max[a] + 2.0f * p->rbf_radius;
+    lb[a] = p->aabb_min[a] - 2.0f * p->rbf_radius;
+  }
+  orc_ray ray;
+  float dir[3];
+  for (int a = 0; a < 3; ++a) {
+    ray.o[a] = p->cam_pos[a];
+    dir[a] = (p->cam_dir00[a] + sx * p->cam_du[a]) + sy * p->cam_dv[a];
+  }
+  v3_normalize(dir, ray.d);
+  ray.tmin = 0.0f;
+  ray.tmax = 10000.0f;
+  float tenter, texit;
+  aabb_intersect(&ray, lb, rt, &tenter, &texit);
+
+  orc_tracker tr;
+  memset(&tr, 0, sizeof(tr));
+  float rnd[3];
+  int blue = (p->flags & ORC_FLAG_BLUE_NOISE) != 0;
+  if (blue) {
+    rnd[0] = noise_at(p, frame, (uint32_t)px, (uint32_t)py);
+    tr.marching = 1;
+  } else {
+    rnd[0] = orc_lcg_randomf(&rng);
+    tr.marching = 0;
+    tr.rng = rng;
+  }
+  rnd[1] = orc_lcg_randomf(&rng);
+  rnd[2] = orc_lcg_randomf(&rng);
+  tr.i = 0;
+  tr.lhs = 0.0f;
+  tr.random = rnd[0];
+  tr.shadow = 0;
+  float col[4] = {0, 0, 0, 0};
+  *noise_out = rnd[0];
+
+  if (tenter < texit) {
+    ray.tmax = texit;
+    tr.t = tenter + p->unit * rnd[1];
+    track(s, p, &tr, &ray, (p->flags & ORC_FLAG_TRACK_FROM_ENTRY) != 0);
+    float albedo[4] = {tr.albedo[0], tr.albedo[1], tr.albedo[2], tr.albedo[3]};
+    float t = tr.t;
+    float vis = 1.0f;
+    if (albedo[3] > 0.0f && p->light_ambient != 1.0f) {
+      orc_ray sr;
+      for (int a = 0; a < 3; ++a) {
+        sr.o[a] = ray.o[a] + ray.d[a] * t;
+        sr.d[a] = light[a];
+      }
+      sr.tmin = 0.0f;
+      sr.tmax = 10000.0f;
+      float ste, stx;
+      aabb_intersect(&sr, lb, rt, &ste, &stx);
+      sr.tmax = stx;
+      tr.albedo[0] = tr.albedo[1] = tr.albedo[2] = tr.albedo[3] = 0.0f;
+      tr.lhs = 0.0f;
+      tr.shadow = 1;
+      tr.t = blue ? -p->unit * rnd[2] : 0.0f;
+      track(s, p, &tr, &sr, 0);
+      vis = 1.0f - tr.albedo[3];
+    }
+    if (albedo[3] == 1.0f) {
+      for (int c = 0; c < 3; ++c)
+        col[c] = (albedo[c] * vis) * (1.0f - p->light_ambient) + albedo[c] * p->light_ambient;
+      col[3] = 1.0f;
+    }
+  }
+  float bg[4] = {0.0f, 0.0f, 0.0f, 1.0f};
+  over(col, bg, color);
+}
+
+static void render_pixel(const orc_scene *s, const orc_params *p, const float *light, int px,
+                         int py, int w, int h, float *accum, float *image) {
+  size_t ofs = (size_t)py * (size_t)w + (size_t)px;
+  float prev[4] = {accum[4 * ofs], accum[4 * ofs + 1], accum[4 * ofs + 2], accum[4 * ofs + 3]};
+  float fin[4] = {prev[0], prev[1], prev[2], prev[3]};
+  float noise = 0.0f;
+  uint32_t spp = p->spp ? p->spp : 1;
+  for (uint32_t k = 0; k < spp; ++k) {
+    uint32_t frame = (p->frame_id + k) & 0xffffu;
+    uint32_t aid = (p->accum_id + k) & 0xffffu;
+    float color[4];
+    raygen_sample(s, p, light, frame, px, py, w, h, color, &noise);
+    /* deviceCodeRBF.hlsl:326-328 */
+    float fa = (float)aid;
+    float wa = 1.0f / fa, wb = (float)((int)aid - 1) / fa;
+    for (int c = 0; c < 4; ++c) fin[c] = wa * color[c] + wb * prev[c];
+    memcpy(prev, fin, sizeof(prev));
+  }
+  memcpy(accum + 4 * ofs, fin, sizeof(fin));
+  if (p->flags & ORC_FLAG_SHOW_NOISE) {
+    fin[0] = fin[1] = fin[2] = noise;
+    fin[3] = 1.0f;
+  }
+  memcpy(image + 4 * ofs, fin, sizeof(fin));
+}
+
+void orc_render_region(const orc_scene *s, const orc_params *p, int w, int h, int x0, int x1,
+                       int y0, int y1, float *accum, float *image, int nthreads) {
+  float light[3];
+  orc_light_dir(p->light_azimuth, p->light_elevation, light);
+  int nt = nthreads > 0 ? nthreads : g_threads;
+  int rows = y1 - y0, cols = x1 - x0;
+  long total = (long)rows * (long)cols;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nt > 0 ? nt : omp_get_max_threads())
+#endif
+  for (long k = 0; k < total; ++k) {
+    int py = y0 + (int)(k / cols), px = x0 + (int)(k % cols);
+    render_pixel(s, p, light, px, py, w, h, accum, image);
+  }
+  (void)nt;
+}
+
+void orc_render(const orc_scene *s, const orc_params *p, int w, int h, float *accum, float *image,
+                int nthreads) {
+  orc_render_region(s, p, w, h, 0, w, 0, h, accum, image, nthreads);
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* splatting: ParticleSplatRayGen / Intersection / AnyHit (deviceCodeSplat.hlsl:29-193)         */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct {
+  float t;
+  uint32_t id;
+} orc_splat_sample;
+
+static int cmp_splat(const void *a, const void *b) {
+  const orc_splat_sample *x = (const orc_splat_sample *)a, *y = (const orc_splat_sample *)b;
+  if (x->t < y->t) return -1;
+  if (x->t > y->t) return 1;
+  return (x->id < y->id) ? -1 : (x->id > y->id ? 1 : 0);
+}
+
+/* splat radius: the global rbfRadius as in deviceCodeSplat.hlsl:166, or the per-particle radius
+ * in native mode; particles whose radiusmap value is 0 are not splatted */
+static float splat_radius(const orc_scene *s, const orc_params *p, uint64_t i) {
+  if (s->rgeom[i] < 0.0f) return 0.0f;
+  return (p->flags & ORC_FLAG_SPLAT_PARTICLE_RADIUS) ? s->rgeom[i] : p->rbf_radius;
+}
+
+static void splat_pixel(const orc_scene *s, const orc_params *p, int px, int py, int w, int h,
+                        float *image) {
+  float sx = ((float)px + 0.5f + p->jitter_x) / (float)w;
+  float sy = ((float)py + 0.5f + p->jitter_y) / (float)h;
+  float rt[3], lb[3];
+  for (int a = 0; a < 3; ++a) {
+    rt[a] = p->aabb_max[a] + p->rbf_radius;
+    lb[a] = p->aabb_min[a] - p->rbf_radius;
+  }
+  orc_ray ray;
+  float dir[3];
+  for (int a = 0; a < 3; ++a) {
+    ray.o[a] = p->cam_pos[a];
+    dir[a] = (p->cam_dir00[a] + sx * p->cam_du[a]) + sy * p->cam_dv[a];
+  }
+  v3_normalize(dir, ray.d);
+  ray.tmin = 0.0f;
+  ray.tmax = 10000.0f;
+  float tenter, texit;
+  aabb_intersect(&ray, lb, rt, &tenter, &texit);
+  float res[4] = {0, 0, 0, 0};
+  if (tenter < texit) {
+    /* every candidate: t = |c - o|; accept if |c - (o + t d)|^2 < r^2 (:165-179); the slab
+     * condition TMin <= t < TMax is applied per slab below. Particles of leaves whose bounds
+     * box is inactive and particles with radiusmap == 0 are not candidates. */
+    size_t cap = 64, cnt = 0;
+    orc_splat_sample *cand = (orc_splat_sample *)malloc(cap * sizeof(orc_splat_sample));
+    for (uint64_t i = 0; i < s->n; ++i) {
+      float r = splat_radius(s, p, i);
+      if (!(r > 0.0f)) continue;
+      const float *c = s->xyzw + 4 * i;
+      float vx = c[0] - ray.o[0], vy = c[1] - ray.o[1], vz = c[2] - ray.o[2];
+      float t = sqrtf((vx * vx + vy * vy) + vz * vz);
+      float sp[3] = {ray.o[0] + t * ray.d[0], ray.o[1] + t * ray.d[1], ray.o[2] + t * ray.d[2]};
+      float ox = c[0] - sp[0], oy = c[1] - sp[1], oz = c[2] - sp[2];
+      if (!(((ox * ox + oy * oy) + oz * oz) < r * r)) continue;
+      if (cnt == cap) {
+        cap *= 2;
+        cand = (orc_splat_sample *)realloc(cand, cap * sizeof(orc_splat_sample));
+      }
+      cand[cnt].t = t;
+      cand[cnt].id = (uint32_t)i;
+      ++cnt;
+    }
+    qsort(cand, cnt, sizeof(orc_splat_sample), cmp_splat);
+    const float per_slab = (float)(15 / 8); /* PARTICLE_BUFFER_SIZE / 8 in integers = 1 */
+    const float spacing = per_slab * p->unit;
+    const float atten = orc_expf(-p->unit * per_slab);
+    float tslab = 0.0f;
+    size_t cursor = 0;
+    while (tslab < texit) {
+      if (res[3] > 0.99f) break;
+      float tmin = orc_maxf(tenter, tslab);
+      float tmax = orc_minf(texit, tslab + spacing);
+      if (tmax > tenter) {
+        while (cursor < cnt && cand[cursor].t < tmin) ++cursor;
+        size_t k = cursor;
+        int taken = 0;
+        while (k < cnt && taken < 15 && cand[k].t < tmax) {
+          const float *P = s->xyzw + 4 * (uint64_t)cand[k].id;
+          float X[3] = {ray.o[0] + ray.d[0] * cand[k].t, ray.o[1] + ray.d[1] * cand[k].t,
+                        ray.o[2] + ray.d[2] * cand[k].t};
+          float dx = X[0] - P[0], dy = X[1] - P[1], dz = X[2] - P[2];
+          float dist = sqrtf((dx * dx + dy * dy) + dz * dz);
+          float r = splat_radius(s, p, cand[k].id);
+          float q = (dist * 3.0f) / r;
+          float drbf = orc_expf(-0.5f * (q * q));
+          float col[4];
+          if (p->flags & ORC_FLAG_VISUALIZE_ATTRIBUTES) {
+            for (int c = 0; c < 4; ++c) col[c] = orc_tex_sample(s->color, s->nc, 4, c, P[3]);
+            drbf = orc_tex_sample(s->density, s->nd, 1, 0, drbf);
+            col[3] = col[3] * drbf;
+          } else {
+            for (int c = 0; c < 3; ++c) col[c] = orc_tex_sample(s->color, s->nc, 4, c, drbf);
+            col[3] = orc_tex_sample(s->density, s->nd, 1, 0, drbf);
+          }
+          col[3] = col[3] * atten;
+          float nr[4];
+          over(res, col, nr);
+          memcpy(res, nr, sizeof(res));
+          ++k;
+          ++taken;
+        }
+      }
+      tslab = tslab + spacing;
+    }
+    free(cand);
+  }
+  float bg[4] = {0.0f, 0.0f, 0.0f, 1.0f};
+  float out[4];
+  over(res, bg, out);
+  memcpy(image + 4 * ((size_t)py * (size_t)w + (size_t)px), out, sizeof(out));
+}
+
+void orc_render_splat(const orc_scene *s, const orc_params *p, int w, int h, float *image,
+                      int nthreads) {
+  int nt = nthreads > 0 ? nthreads : g_threads;
+  long total = (long)w * (long)h;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nt > 0 ? nt : omp_get_max_threads())
+#endif
+  for (long k = 0; k < total; ++k) splat_pixel(s, p, (int)(k % w), (int)(k / w), w, h, image);
+  (void)nt;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* TAA resolve (deviceCodeCommon.hlsl:27-43, 67-115)                                           */
+/* ------------------------------------------------------------------------------------------ */
+
+static void rgb2ycocg(const float *c, float *o) {
+  float co = c[0] - c[2];
+  float t = c[2] + co / 2.0f;
+  float cg = c[1] - t;
+  float y = t + cg / 2.0f;
+  o[0] = y; o[1] = co; o[2] = cg;
+}
+static void ycocg2rgb(const float *c, float *o) {
+  float t = c[0] - c[2] / 2.0f;
+  float g = c[2] + t;
+  float b = t - c[1] / 2.0f;
+  float r = c[1] + b;
+  o[0] = r; o[1] = g; o[2] = b;
+}
+
+static uint8_t unorm8(float v) {
+  if (!(v > 0.0f)) v = 0.0f;
+  if (v > 1.0f) v = 1.0f;
+  return (uint8_t)(v * 255.0f + 0.5f);
+}
+
+void orc_taa(const float *image, const float *prev, float *taa, uint32_t *bgra, int w, int h,
+             int disable) {
+  for (int py = 0; py < h; ++py) {
+    for (int px = 0; px < w; ++px) {
+      size_t ofs = (size_t)py * (size_t)w + (size_t)px;
+      const float *center = image + 4 * ofs;
+      float pix[4];
+      if (!disable) {
+        float mn[3], mx[3];
+        rgb2ycocg(center, mn);
+        rgb2ycocg(center, mx);
+        for (int iy = -1; iy <= 1; ++iy) {
+          for (int ix = -1; ix <= 1; ++ix) {
+            if (ix == 0 && iy == 0) continue;
+            int qx = px + ix, qy = py + iy;
+            if (qx < 0) qx = 0;
+            if (qx > w - 1) qx = w - 1;
+            if (qy < 0) qy = 0;
+            if (qy > h - 1) qy = h - 1;
+            float y[3];
+            rgb2ycocg(image + 4 * ((size_t)qy * (size_t)w + (size_t)qx), y);
+            for (int c = 0; c < 3; ++c) {
+              mn[c] = orc_minf(mn[c], y[c]);
+              mx[c] = orc_maxf(mx[c], y[c]);
+            }
+          }
+        }
+        float old[4] = {prev[4 * ofs], prev[4 * ofs + 1], prev[4 * ofs + 2], prev[4 * ofs + 3]};
+        float y[3], rgb[3];
+        rgb2ycocg(old, y);
+        for (int c = 0; c < 3; ++c) y[c] = orc_maxf(y[c], mn[c]);
+        ycocg2rgb(y, rgb);
+        rgb2ycocg(rgb, y);
+        for (int c = 0; c < 3; ++c) y[c] = orc_minf(y[c], mx[c]);
+        ycocg2rgb(y, rgb);
+        old[0] = rgb[0]; old[1] = rgb[1]; old[2] = rgb[2];
+        for (int c = 0; c < 4; ++c) pix[c] = old[c] + 0.2f * (center[c] - old[c]);
+        memcpy(taa + 4 * ofs, pix, sizeof(pix));
+      } else {
+        memcpy(pix, center, sizeof(pix));
+      }
+      if (bgra) {
+        /* GUI layer is empty: over((0,0,0,0), pixel) (:193-195), then BGRA8 */
+        float gui[4] = {0, 0, 0, 0}, o[4];
+        over(gui, pix, o);
+        bgra[ofs] = (uint32_t)unorm8(o[2]) | ((uint32_t)unorm8(o[1]) << 8) |
+                    ((uint32_t)unorm8(o[0]) << 16) | ((uint32_t)unorm8(o[3]) << 24);
+      }
+    }
+  }
+}

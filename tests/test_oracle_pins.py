@@ -1,0 +1,170 @@
+"""The oracle is pinned before it is trusted: Hilbert encoder and RNG against golden vectors made
+by the reference's own hilbert.h / rng.h (and live against that library when it is present),
+the deterministic exp/log/pow against float64, and the renderer restatement against closed-form
+known answers (single particle densities, empty scene, fixed points)."""
+import ctypes
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = json.load(open(os.path.join(ROOT, "tests", "golden", "hilbert_rng.json")))
+
+
+def test_hilbert_c2i_golden(orc):
+    L = orc.lib()
+    bad = 0
+    for nd, nb, x, y, z, idx in GOLD["hilbert_c2i"]:
+        c = np.array([x, y, z], np.uint64)
+        bad += L.orc_hilbert_c2i(nd, nb, c.ctypes.data) != idx
+    assert bad == 0
+    assert len(GOLD["hilbert_c2i"]) >= 4096 + 4000
+
+
+def test_hilbert_i2c_golden_and_roundtrip(orc):
+    L = orc.lib()
+    for nd, nb, idx, x, y, z in GOLD["hilbert_i2c"]:
+        c = np.zeros(3, np.uint64)
+        L.orc_hilbert_i2c(nd, nb, idx, c.ctypes.data)
+        assert list(c) == [x, y, z]
+        assert L.orc_hilbert_c2i(nd, nb, c.ctypes.data) == idx
+
+
+def test_hilbert_is_a_curve(orc):
+    """consecutive indices map to unit-distance neighbours over the whole 2^12 grid"""
+    L = orc.lib()
+    prev = None
+    seen = set()
+    for i in range(4096):
+        c = np.zeros(3, np.uint64)
+        L.orc_hilbert_i2c(3, 4, i, c.ctypes.data)
+        t = tuple(int(v) for v in c)
+        seen.add(t)
+        if prev is not None:
+            assert sum(abs(a - b) for a, b in zip(t, prev)) == 1
+        prev = t
+    assert len(seen) == 4096
+
+
+def test_rng_golden(orc):
+    L = orc.lib()
+    for e in GOLD["rng"]:
+        s = L.orc_get_rng(e["frame"], e["pixel"][0], e["pixel"][1], e["width"])
+        assert s == e["seed"]
+        st = ctypes.c_uint32(s)
+        for want_state, want_f in zip(e["states"], e["floats"]):
+            f = L.orc_lcg_randomf(ctypes.byref(st))
+            assert st.value == want_state
+            assert float(np.float32(f)).hex() == want_f
+    for h, k, m, fin in GOLD["murmur"]:
+        assert L.orc_murmur_mix(h, k) == m
+        assert L.orc_murmur_finalize(h) == fin
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libaarbf_ref.so")),
+                    reason="reference tree not present (golden vectors still pin the oracle)")
+def test_hilbert_live_reference(orc):
+    R = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libaarbf_ref.so"))
+    R.ref_hilbert_c2i.restype = ctypes.c_ulonglong
+    L = orc.lib()
+    rng = np.random.default_rng(5)
+    for nd, nb in [(3, 16), (2, 8), (4, 5), (3, 21), (2, 32), (3, 1)]:
+        for _ in range(500):
+            c = rng.integers(0, 2 ** nb, size=nd).astype(np.uint64)
+            assert L.orc_hilbert_c2i(nd, nb, c.ctypes.data) == R.ref_hilbert_c2i(nd, nb, ctypes.c_void_p(c.ctypes.data))
+
+
+def test_det_math_accuracy(orc):
+    L = orc.lib()
+    rng = np.random.default_rng(0)
+    xs = rng.uniform(1e-30, 10.0, 5000).astype(np.float32)
+    for x in xs:
+        g = L.orc_logf(float(x))
+        r = math.log(float(x))
+        assert abs(g - r) <= 3 * np.spacing(np.float32(abs(r))) + 1e-12
+    for x in rng.uniform(-100, 80, 5000).astype(np.float32):
+        g = L.orc_expf(float(x))
+        r = math.exp(float(x))
+        if r > 1.2e-38:
+            assert abs(g - r) <= 1.5 * float(np.spacing(np.float32(r)))
+    assert L.orc_expf(0.0) == 1.0 and L.orc_logf(1.0) == 0.0
+    assert L.orc_expf(-200.0) == 0.0 and math.isinf(L.orc_expf(100.0))
+    assert math.isinf(L.orc_logf(0.0)) and L.orc_powf(0.0, 2.2) == 0.0
+
+
+def _one_particle_scene(orc, p=(0.5, 0.5, 0.5, 0.5), r=0.1, alpha=1.0):
+    cm = np.tile(np.array([[0.2, 0.4, 0.8, alpha]], np.float32), (4, 1))
+    tf = (cm, np.ones(4, np.float32), np.linspace(0, 1, 4).astype(np.float32))
+    xyzw = np.array([p], np.float32)
+    return orc.Scene(xyzw, None, np.zeros(1, np.uint64), 1, r, tf)
+
+
+def test_single_particle_density_kat(orc):
+    """D(p) = alpha^3; D at distance d = alpha^3 exp(-4.5 (d/r)^2); D = 0 at and beyond r
+    (evaluate_rbf with sigma 3, sharedCode.h:137-140; any-hit sum deviceCodeRBF.hlsl:375)"""
+    for alpha in (1.0, 0.5):
+        s = _one_particle_scene(orc, alpha=alpha)
+        c, acc = s.point_query([0.5, 0.5, 0.5])
+        assert c == 1
+        assert abs(acc[0] * 2.0 ** -40 - alpha ** 3) < 1e-6
+        for d in (0.03, 0.07, 0.0999):
+            c, acc = s.point_query([0.5 + d, 0.5, 0.5])
+            want = alpha ** 3 * math.exp(-4.5 * (d / 0.1) ** 2)
+            assert c == 1 and abs(acc[0] * 2.0 ** -40 - want) < 2e-6 * max(1, want)
+        for d in (0.1, 0.2):
+            c, acc = s.point_query([0.5 + d, 0.5, 0.5])
+            assert c == 0 and acc[0] == 0
+    # a transparent particle is never counted (deviceCodeRBF.hlsl:369-372)
+    s = _one_particle_scene(orc, alpha=0.0)
+    assert s.point_query([0.5, 0.5, 0.5])[0] == 0
+
+
+def test_point_query_bvh_matches_brute_force(orc):
+    rng = np.random.default_rng(3)
+    n = 3000
+    xyzw = np.concatenate([rng.uniform(0, 1, (n, 3)), rng.uniform(0, 1, (n, 1))], 1).astype(np.float32)
+    dom = orc.domain([xyzw])
+    cm = np.stack([np.linspace(0, 1, 64)] * 3 + [np.linspace(0.1, 1, 64)], 1).astype(np.float32)
+    tf = (cm, np.linspace(0.5, 1, 64).astype(np.float32), np.linspace(0, 1, 64).astype(np.float32))
+    for ppl in (1, 3, 8):
+        s, _, _ = orc.build_scene(xyzw, None, dom, ppl, 0.05, tf)
+        for q in rng.uniform(-0.05, 1.05, (300, 3)).astype(np.float32):
+            a = s.point_query(q)
+            b = s.point_query(q, brute=True)
+            assert a[0] == b[0] and np.array_equal(a[1], b[1])
+
+
+def _tf_default(orc):
+    import aarbf
+    return orc.tf_from_rgba8(*aarbf.default_transfer_functions_rgba8())
+
+
+def test_empty_scene_renders_background(orc):
+    s = orc.Scene(np.zeros((0, 4), np.float32), None, np.zeros(0, np.uint64), 1, 0.1, _tf_default(orc))
+    from aarbf import RenderParams
+    rp = RenderParams(cam_pos=(0.5, 0.5, -2), cam_dir00=(-0.5, -0.5, 1), cam_du=(1, 0, 0), cam_dv=(0, 1, 0),
+                      unit=0.01, rbf_radius=0.1)
+    acc, img = s.render(orc.params_from(rp), 16, 16)
+    assert np.array_equal(img, np.tile(np.array([0, 0, 0, 1], np.float32), (16, 16, 1)))
+
+
+def test_taa_constant_image_is_fixed_point(orc):
+    img = np.tile(np.array([0.3, 0.6, 0.2, 1.0], np.float32), (8, 8, 1))
+    out, bgra = orc.taa(img, img.copy())
+    assert np.allclose(out, img, atol=1e-6)
+    assert (bgra == ((255 << 24) | (int(0.3 * 255 + .5) << 16) | (int(0.6 * 255 + .5) << 8) | int(0.2 * 255 + .5))).all()
+
+
+def test_sort_tie_break(orc):
+    """equal Hilbert keys are ordered by (x, y, z, w) then input index"""
+    xyzw = np.array([[0.5, 0.5, 0.5, 0.9], [0.5, 0.5, 0.5, 0.1], [0.0, 0.0, 0.0, 0.0], [1, 1, 1, 1],
+                     [0.5, 0.5, 0.5, 0.1]], np.float32)
+    dom = orc.domain([xyzw])
+    k = orc.hilbert_keys(xyzw, dom)
+    perm = orc.sort_perm(k, xyzw)
+    order = [int(i) for i in perm]
+    pos = {i: order.index(i) for i in range(5)}
+    assert pos[1] < pos[4] < pos[0]
