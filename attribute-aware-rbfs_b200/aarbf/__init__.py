@@ -30,6 +30,7 @@ FLAG_VISUALIZE_ATTRIBUTES = 1 << 2
 FLAG_TRACK_FROM_ENTRY = 1 << 3
 FLAG_DENSITY_LINEAR = 1 << 4
 FLAG_SPLAT_PARTICLE_RADIUS = 1 << 5
+FLAG_MAJORANT_TRACKING = 1 << 6
 
 TRAVERSAL_STAGED = 0
 TRAVERSAL_POINT = 1
@@ -50,7 +51,7 @@ EXPORTED_SYMBOLS = (
     "aarbf_series_num_frames", "aarbf_series_frame", "aarbf_series_free", "aarbf_series_save",
     "aarbf_get_num_particles", "aarbf_get_hilbert_keys", "aarbf_get_sorted_particles",
     "aarbf_get_prepass", "aarbf_get_bvh", "aarbf_device_alloc", "aarbf_device_free",
-    "aarbf_memcpy", "aarbf_memset", "aarbf_render_count",
+    "aarbf_memcpy", "aarbf_memset", "aarbf_render_count", "aarbf_set_opacity_floor",
 )
 
 
@@ -73,7 +74,8 @@ class Params(ctypes.Structure):
         ("rbf_radius", ctypes.c_float), ("unit", ctypes.c_float),
         ("aabb_min", ctypes.c_float * 3), ("aabb_max", ctypes.c_float * 3),
         ("density_gain", ctypes.c_float), ("jitter_x", ctypes.c_float), ("jitter_y", ctypes.c_float),
-        ("traversal", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3),
+        ("traversal", ctypes.c_int32), ("density_scale", ctypes.c_float), ("bin_length", ctypes.c_float),
+        ("candidate_cap", ctypes.c_int32),
     ]
 
 
@@ -112,7 +114,8 @@ def _load():
         "aarbf_get_hilbert_keys": [P, P, P],
         "aarbf_get_sorted_particles": [P, P],
         "aarbf_get_prepass": [P, P, P, P],
-        "aarbf_get_bvh": [P, P, P, P, P, P],
+        "aarbf_get_bvh": [P, P, P, P, P, P, P],
+        "aarbf_set_opacity_floor": [P, f32],
         "aarbf_get_version": [ctypes.POINTER(i32), ctypes.POINTER(i32)],
         "aarbf_device_alloc": [P, ctypes.c_size_t, ctypes.POINTER(P)],
         "aarbf_device_free": [P, P],
@@ -237,6 +240,9 @@ class RenderParams:
     jitter_x: float = 0.0
     jitter_y: float = 0.0
     traversal: int = TRAVERSAL_STAGED
+    density_scale: float = 0.0
+    bin_length: float = 0.0
+    candidate_cap: int = 0
 
     def to_c(self) -> Params:
         p = Params()
@@ -249,6 +255,8 @@ class RenderParams:
         p.rbf_radius, p.unit = self.rbf_radius, self.unit
         p.density_gain, p.jitter_x, p.jitter_y = self.density_gain, self.jitter_x, self.jitter_y
         p.traversal = int(self.traversal)
+        p.density_scale, p.bin_length = self.density_scale, self.bin_length
+        p.candidate_cap = int(self.candidate_cap)
         return p
 
 
@@ -345,12 +353,14 @@ class Context:
 
     def render_count(self, params: RenderParams, width: int, height: int, accum=None, image=None,
                      stream=None):
-        """render + accounting: (particles met by traversed ray segments, BVH node visits)"""
+        """render + accounting: dict of the AARBF_COUNT_SLOTS counters (include/aarbf.h)"""
         p = params.to_c() if isinstance(params, RenderParams) else params
-        c = np.zeros(2, np.uint64)
+        c = np.zeros(10, np.uint64)
         self._check(self._lib.aarbf_render_count(self._h, ctypes.byref(p), int(width), int(height),
                                                  _ptr(accum), _ptr(image), _ptr(c), _stream_ptr(stream)))
-        return int(c[0]), int(c[1])
+        names = ("segment_particles", "segment_nodes", "steps", "stagings", "staging_overflows",
+                 "point_queries", "candidate_checks", "particle_evals", "staging_nodes", "point_nodes")
+        return {k: int(v) for k, v in zip(names, c)}
 
     def render_splat(self, params: RenderParams, width: int, height: int, image=None, stream=None):
         p = params.to_c() if isinstance(params, RenderParams) else params
@@ -417,10 +427,14 @@ class Context:
         right = np.zeros(ni, np.uint32)
         nb = np.zeros((ni, 6), np.float32)
         lb = np.zeros((nl, 6), np.float32)
+        le = np.zeros((nl, 6), np.float32)
         rb = np.zeros(6, np.float32)
         self._check(self._lib.aarbf_get_bvh(self._h, _ptr(left), _ptr(right), _ptr(nb), _ptr(lb),
-                                            _ptr(rb)))
-        return left, right, nb, lb, rb
+                                            _ptr(le), _ptr(rb)))
+        return left, right, nb, lb, le, rb
+
+    def set_opacity_floor(self, alpha_floor: float):
+        self._check(self._lib.aarbf_set_opacity_floor(self._h, float(alpha_floor)))
 
 
 def load_series(path: str):

@@ -130,17 +130,23 @@ def orbit_camera(center=(0.5, 0.5, 0.5), distance: float = 2.5, azimuth_deg: flo
 
 
 def native_params(cam, width: int, height: int, rbf_radius: float, unit: float, density_scale: float,
-                  dom, spp: int = 1, frame_id: int = 0, traversal: int = 0, marching: bool = False):
+                  dom, spp: int = 1, frame_id: int = 0, traversal: int = 0, marching: bool = False,
+                  majorant: bool = False, bin_length: float = None):
     """Render parameters of the benchmark configurations (native mode: per-particle radii, fp32
-    transfer function, density = min(density_scale * D * unit, 1) per unit step, tracking from the
-    volume entry)."""
-    from . import camera, FLAG_BLUE_NOISE
+    transfer function). Plain form: delta tracking with the global majorant 1/unit, density
+    min(density_scale * D * unit, 1) per unit step, from the volume entry. Majorant form: delta
+    tracking of extinction density_scale * D with per-bin majorants (bins of bin_length, default
+    4 units)."""
+    from . import camera, FLAG_BLUE_NOISE, FLAG_MAJORANT_TRACKING
     pos, d00, du, dv = camera(cam[0], cam[1], cam[2], cam[3], width, height)
     flags = FLAG_VISUALIZE_ATTRIBUTES | FLAG_DENSITY_LINEAR | FLAG_TRACK_FROM_ENTRY | FLAG_SPLAT_PARTICLE_RADIUS
     if marching:
         flags |= FLAG_BLUE_NOISE
+    if majorant:
+        flags |= FLAG_MAJORANT_TRACKING
     return RenderParams(cam_pos=pos, cam_dir00=d00, cam_du=du, cam_dv=dv, aabb_min=dom[0:3],
                         aabb_max=dom[3:6], rbf_radius=rbf_radius, unit=unit, accum_id=1,
                         frame_id=frame_id, spp=spp, flags=flags, light_ambient=0.5,
                         density_gain=float(np.float32(density_scale) * np.float32(unit)),
-                        traversal=traversal)
+                        traversal=traversal, density_scale=float(density_scale),
+                        bin_length=float(np.float32(bin_length if bin_length else 4.0 * unit)))

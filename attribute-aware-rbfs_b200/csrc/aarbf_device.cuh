@@ -32,6 +32,8 @@ enum : uint32_t {
   kFlagTrackFromEntry = 1u << 3,
   kFlagDensityLinear = 1u << 4,
   kFlagSplatParticleRadius = 1u << 5,
+  kFlagMajorantTracking = 1u << 6,
+  kFlagCostImage = 1u << 7,
 };
 
 // Internal BVH node: the boxes of both children live in the parent, so a traversal step reads

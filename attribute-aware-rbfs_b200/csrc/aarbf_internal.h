@@ -40,7 +40,8 @@ struct SceneView {
   const float4* w4;    // a^3, pow(rgb, 2.2) a^3
   const float4* xyzw;  // sorted particles (attribute normalised)
   const float* rgeom;  // bounds radius, -1 = skipped by the bounds program
-  const Node* nodes;
+  const Node* nodes;      // traversal bounds (particles that can be hit)
+  const Node* nodes_ref;  // reference bounds (splatting)
   const float4* tf_color;
   const float* tf_density;
   uint64_t n;
@@ -70,6 +71,9 @@ struct RenderLaunch {
   int traversal;
   float splat_rmax;                // largest splat radius of the scene
   unsigned long long* counters;    // count mode: [particles on traversed segments, node visits]
+  float density_scale, bin_length; // majorant tracking
+  uint32_t* work_counter;          // persistent kernel: next pixel tile item (zeroed per launch)
+  int candidate_cap;               // staging buffer depth per ray (template instance)
 };
 
 // launchers (defined in the .cu files)
@@ -90,13 +94,14 @@ cudaError_t launch_gather_normalize(const float4* in, const float* radii_in, con
                                     uint64_t n, float amin, float amax, float4* out,
                                     float* radii_out, cudaStream_t st);
 cudaError_t launch_prepass(const float4* xyzw, const float* radii, uint64_t n, const float4* tf_color,
-                           int nc, const float* tf_radius, int nr, float rbf_radius, float4* rec0,
-                           float4* w4, float* rgeom, cudaStream_t st);
+                           int nc, const float* tf_radius, int nr, float rbf_radius, float alpha_floor,
+                           float4* rec0, float4* w4, float* rgeom, cudaStream_t st);
 cudaError_t launch_karras(const uint64_t* sorted_keys, uint64_t n, uint32_t ppl, uint32_t nleaves,
-                          Node* nodes, uint32_t* leaf_parent, cudaStream_t st);
+                          Node* nodes, Node* nodes_ref, uint32_t* leaf_parent, cudaStream_t st);
 cudaError_t launch_refit(const float4* rec0, const float* rgeom, uint64_t n, uint32_t ppl,
-                         uint32_t nleaves, Node* nodes, const uint32_t* leaf_parent, uint32_t* counters,
-                         float* leaf_box, float* root_box, cudaStream_t st);
+                         uint32_t nleaves, Node* nodes, Node* nodes_ref, const uint32_t* leaf_parent,
+                         uint32_t* counters, float* leaf_box, float* leaf_eff, float* root_box,
+                         cudaStream_t st);
 cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st);
 cudaError_t launch_splat(const RenderLaunch& L, cudaStream_t st);
 cudaError_t launch_taa(const float4* image, const float4* prev, float4* taa, uint32_t* bgra, int w,
@@ -117,7 +122,9 @@ struct aarbf_ctx {
   // sort
   aarbf::DevBuf keys, keys_alt, perm, perm_alt, hist, tmp_keys, flag;
   // sorted scene
-  aarbf::DevBuf xyzw, radii, rec0, w4, rgeom, nodes, leaf_parent, counters, leaf_box, root_box;
+  aarbf::DevBuf xyzw, radii, rec0, w4, rgeom, nodes, nodes_ref, leaf_parent, counters, leaf_box, leaf_eff,
+      root_box;
+  float alpha_floor = 0.0f;  // opacity below this counts as transparent
   aarbf::DevBuf sorted_keys;  // Hilbert keys in sorted order
   uint32_t ppl = 1, nleaves = 0;
   float rbf_radius = 0.0f;
@@ -133,7 +140,7 @@ struct aarbf_ctx {
   // framebuffers owned by the context
   aarbf::DevBuf fb_accum, fb_image;
   int fb_w = 0, fb_h = 0;
-  // status word
-  aarbf::DevBuf status;
+  // status word, persistent-kernel work counter
+  aarbf::DevBuf status, work;
   float max_radius = 0.0f;
 };

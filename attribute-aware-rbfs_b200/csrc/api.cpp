@@ -117,11 +117,11 @@ aarbf_status run_refit(aarbf_ctx* ctx, cudaStream_t st) {
   if (s != AARBF_OK) return s;
   CK(launch_prepass(ctx->xyzw.as<float4>(), ctx->has_radii ? ctx->radii.as<float>() : nullptr, n,
                     ctx->tf_color.as<float4>(), ctx->nc, ctx->tf_radius.as<float>(), ctx->nr, ctx->rbf_radius,
-                    ctx->rec0.as<float4>(), ctx->w4.as<float4>(), ctx->rgeom.as<float>(), st),
+                    ctx->alpha_floor, ctx->rec0.as<float4>(), ctx->w4.as<float4>(), ctx->rgeom.as<float>(), st),
      "prepass");
   CK(launch_refit(ctx->rec0.as<float4>(), ctx->rgeom.as<float>(), n, ctx->ppl, ctx->nleaves, ctx->nodes.as<Node>(),
-                  ctx->leaf_parent.as<uint32_t>(), ctx->counters.as<uint32_t>(), ctx->leaf_box.as<float>(),
-                  ctx->root_box.as<float>(), st),
+                  ctx->nodes_ref.as<Node>(), ctx->leaf_parent.as<uint32_t>(), ctx->counters.as<uint32_t>(),
+                  ctx->leaf_box.as<float>(), ctx->leaf_eff.as<float>(), ctx->root_box.as<float>(), st),
      "refit");
   if (ctx->nleaves) {
     CK(cudaMemcpyAsync(ctx->root_box_host, ctx->root_box.ptr, 6 * sizeof(float), cudaMemcpyDeviceToHost, st),
@@ -168,6 +168,7 @@ aarbf_status fill_launch(aarbf_ctx* ctx, const aarbf_params* p, int w, int h, fl
   s.xyzw = ctx->xyzw.as<float4>();
   s.rgeom = ctx->rgeom.as<float>();
   s.nodes = ctx->nodes.as<Node>();
+  s.nodes_ref = ctx->nodes_ref.as<Node>();
   s.tf_color = ctx->tf_color.as<float4>();
   s.tf_density = ctx->tf_density.as<float>();
   s.n = ctx->n;
@@ -211,7 +212,16 @@ aarbf_status fill_launch(aarbf_ctx* ctx, const aarbf_params* p, int w, int h, fl
   L.status = ctx->status.as<uint32_t>();
   L.traversal = p->traversal;
   L.splat_rmax = (p->flags & kFlagSplatParticleRadius) ? ctx->max_radius : p->rbf_radius;
+  L.density_scale = p->density_scale;
+  L.bin_length = p->bin_length;
+  L.candidate_cap = p->candidate_cap ? p->candidate_cap : 32;
+  if (L.candidate_cap != 16 && L.candidate_cap != 32 && L.candidate_cap != 64 && L.candidate_cap != 128)
+    return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "candidate_cap must be 16, 32, 64 or 128");
   if (!(p->unit > 0.0f)) return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "unit must be > 0");
+  if ((p->flags & kFlagMajorantTracking) && !(p->bin_length > 0.0f && p->density_scale >= 0.0f))
+    return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "majorant tracking needs bin_length > 0, density_scale >= 0");
+  if (!ctx->work.ptr) CK(ctx->work.reserve(256), "work counter");
+  L.work_counter = ctx->work.as<uint32_t>();
   return AARBF_OK;
 }
 
@@ -277,9 +287,10 @@ aarbf_status aarbf_destroy(aarbf_ctx* ctx) {
   cudaSetDevice(ctx->device);
   DevBuf* bufs[] = {&ctx->in_xyzw, &ctx->in_radii, &ctx->keys, &ctx->keys_alt, &ctx->perm, &ctx->perm_alt,
                     &ctx->hist, &ctx->tmp_keys, &ctx->flag, &ctx->xyzw, &ctx->radii, &ctx->rec0, &ctx->w4,
-                    &ctx->rgeom, &ctx->nodes, &ctx->leaf_parent, &ctx->counters, &ctx->leaf_box, &ctx->root_box,
+                    &ctx->rgeom, &ctx->nodes, &ctx->nodes_ref, &ctx->leaf_eff, &ctx->leaf_parent, &ctx->counters,
+                    &ctx->leaf_box, &ctx->root_box,
                     &ctx->sorted_keys, &ctx->tf_color, &ctx->tf_radius, &ctx->tf_density, &ctx->noise,
-                    &ctx->fb_accum, &ctx->fb_image, &ctx->status};
+                    &ctx->fb_accum, &ctx->fb_image, &ctx->status, &ctx->work};
   for (DevBuf* b : bufs) b->release();
   delete ctx;
   return AARBF_OK;
@@ -463,6 +474,8 @@ aarbf_status aarbf_build(aarbf_ctx* ctx, float rbf_radius, uint32_t ppl, void* s
   if (ctx->has_radii) CK(ctx->radii.reserve(4 * nn), "alloc");
   const uint64_t nl = ctx->nleaves ? ctx->nleaves : 1;
   CK(ctx->nodes.reserve(sizeof(Node) * nl), "alloc");
+  CK(ctx->nodes_ref.reserve(sizeof(Node) * nl), "alloc");
+  CK(ctx->leaf_eff.reserve(24 * nl), "alloc");
   CK(ctx->leaf_parent.reserve(4 * nl), "alloc");
   CK(ctx->counters.reserve(4 * nl), "alloc");
   CK(ctx->leaf_box.reserve(24 * nl), "alloc");
@@ -517,7 +530,7 @@ aarbf_status aarbf_build(aarbf_ctx* ctx, float rbf_radius, uint32_t ppl, void* s
                                dom[6], dom[7], ctx->xyzw.as<float4>(), ctx->radii.as<float>(), st),
        "gather");
     CK(launch_karras(ctx->sorted_keys.as<uint64_t>(), n, ppl, ctx->nleaves, ctx->nodes.as<Node>(),
-                     ctx->leaf_parent.as<uint32_t>(), st),
+                     ctx->nodes_ref.as<Node>(), ctx->leaf_parent.as<uint32_t>(), st),
        "karras");
   }
   memcpy(ctx->dom, dom, sizeof(dom));
@@ -589,17 +602,16 @@ aarbf_status aarbf_render_count(aarbf_ctx* ctx, const aarbf_params* p, int w, in
   if (s != AARBF_OK) return s;
   cudaStream_t st = (cudaStream_t)stream;
   DevBuf c;
-  CK(c.reserve(64), "count alloc");
-  cudaError_t e = cudaMemsetAsync(c.ptr, 0, 64, st);
+  unsigned long long h2[AARBF_COUNT_SLOTS] = {};
+  CK(c.reserve(sizeof(h2)), "count alloc");
+  cudaError_t e = cudaMemsetAsync(c.ptr, 0, sizeof(h2), st);
   L.counters = c.as<unsigned long long>();
   if (e == cudaSuccess) e = launch_render(L, st);
-  unsigned long long h2[2] = {0, 0};
   if (e == cudaSuccess) e = cudaMemcpyAsync(h2, c.ptr, sizeof(h2), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   c.release();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "render count");
-  counts[0] = h2[0];
-  counts[1] = h2[1];
+  for (int k = 0; k < AARBF_COUNT_SLOTS; ++k) counts[k] = h2[k];
   return AARBF_OK;
 }
 
@@ -776,8 +788,19 @@ aarbf_status aarbf_get_prepass(aarbf_ctx* ctx, float* rec0, float* w4, float* rg
   return AARBF_OK;
 }
 
+aarbf_status aarbf_set_opacity_floor(aarbf_ctx* ctx, float alpha_floor) {
+  if (!ctx) return AARBF_ERR_INVALID_ARGUMENT;
+  if (!(alpha_floor >= 0.0f && alpha_floor <= 1.0f))
+    return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "opacity floor must lie in [0, 1]");
+  if (alpha_floor != ctx->alpha_floor) {
+    ctx->alpha_floor = alpha_floor;
+    ctx->built = false;
+  }
+  return AARBF_OK;
+}
+
 aarbf_status aarbf_get_bvh(aarbf_ctx* ctx, uint32_t* left, uint32_t* right, float* node_box, float* leaf_box,
-                           float* root_box) {
+                           float* leaf_eff, float* root_box) {
   if (!ctx) return AARBF_ERR_INVALID_ARGUMENT;
   if (!ctx->built) return fail(ctx, AARBF_ERR_NOT_READY, "not built");
   cudaSetDevice(ctx->device);
@@ -797,6 +820,7 @@ aarbf_status aarbf_get_bvh(aarbf_ctx* ctx, uint32_t* left, uint32_t* right, floa
     }
   }
   if (leaf_box && L) CK(cudaMemcpy(leaf_box, ctx->leaf_box.ptr, 24 * (size_t)L, cudaMemcpyDeviceToHost), "leaf box");
+  if (leaf_eff && L) CK(cudaMemcpy(leaf_eff, ctx->leaf_eff.ptr, 24 * (size_t)L, cudaMemcpyDeviceToHost), "leaf box");
   if (root_box) memcpy(root_box, ctx->root_box_host, 6 * sizeof(float));
   return AARBF_OK;
 }

@@ -1,7 +1,13 @@
 // lbvh.cu -- the reference's bounds program (deviceCodeBounds.hlsl:29-82) turned into an LBVH
 // builder: per-particle shading prepass, Karras (HPG 2012) radix tree over the leaf clusters'
-// Hilbert keys, and a bottom-up refit that computes the leaf boxes exactly as GenRBFBounds
-// does and unions them upwards with atomic arrival counters.
+// Hilbert keys, and a bottom-up refit with atomic arrival counters.
+//
+// The refit produces two box sets over one topology:
+//  - reference bounds: leaf boxes exactly as GenRBFBounds computes them (radius from the radius
+//    map, every particle whose radius-map value is non-zero) -- the bounds output, and the tree
+//    the splat kernel traverses (splatting ignores opacity, deviceCodeSplat.hlsl:156-187);
+//  - traversal bounds: leaf boxes over the particles that can be hit (r_eval > 0), the tree the
+//    tracking kernels traverse. Particles outside it never contribute, so results are unchanged.
 #include "aarbf_internal.h"
 
 namespace aarbf {
@@ -11,11 +17,12 @@ namespace {
 inline unsigned blocks_for(uint64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 // radius (deviceCodeRBF.hlsl:349-351, deviceCodeBounds.hlsl:59) and the per-particle any-hit
-// weights (deviceCodeRBF.hlsl:366-376), evaluated once per particle instead of once per hit
+// weights (deviceCodeRBF.hlsl:366-376), evaluated once per particle instead of once per hit.
+// Opacity 0, or below alpha_floor, marks a particle transparent (deviceCodeRBF.hlsl:369-372).
 __global__ void k_prepass(const float4* __restrict__ xyzw, const float* __restrict__ radii, uint64_t n,
                           const float4* __restrict__ tf_color, int nc, const float* __restrict__ tf_radius,
-                          int nr, float rbf_radius, float4* __restrict__ rec0, float4* __restrict__ w4,
-                          float* __restrict__ rgeom) {
+                          int nr, float rbf_radius, float alpha_floor, float4* __restrict__ rec0,
+                          float4* __restrict__ w4, float* __restrict__ rgeom) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   float4 p = __ldg(xyzw + i);
@@ -24,7 +31,7 @@ __global__ void k_prepass(const float4* __restrict__ xyzw, const float* __restri
   float r = base * rp;
   float4 col = tex4(tf_color, nc, p.w);
   rgeom[i] = (rp == 0.0f) ? -1.0f : r;
-  if (col.w == 0.0f) {
+  if (col.w == 0.0f || col.w < alpha_floor) {
     rec0[i] = make_float4(p.x, p.y, p.z, 0.0f);
     w4[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   } else {
@@ -45,7 +52,7 @@ __device__ __forceinline__ int delta(const uint64_t* __restrict__ keys, uint32_t
 
 // leaf l's key is the key of its first particle; equal keys are ordered by leaf index
 __global__ void k_karras(const uint64_t* __restrict__ keys, uint32_t ppl, uint32_t nleaves, Node* nodes,
-                         uint32_t* leaf_parent) {
+                         Node* nodes_ref, uint32_t* leaf_parent) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t L = nleaves;
   if (i >= L - 1) return;
@@ -67,14 +74,19 @@ __global__ void k_karras(const uint64_t* __restrict__ keys, uint32_t ppl, uint32
   int64_t lo = i < j ? i : j, hi = i < j ? j : i;
   uint32_t left = (lo == g) ? ((uint32_t)g | kLeafBit) : (uint32_t)g;
   uint32_t right = (hi == g + 1) ? ((uint32_t)(g + 1) | kLeafBit) : (uint32_t)(g + 1);
-  nodes[i].d.x = left;
-  nodes[i].d.y = right;
-  nodes[i].d.w = 0u;
-  if (i == 0) nodes[0].d.z = 0xffffffffu;
+  Node* trees[2] = {nodes, nodes_ref};
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    Node* nd = trees[t];
+    nd[i].d.x = left;
+    nd[i].d.y = right;
+    nd[i].d.w = 0u;
+    if (i == 0) nd[0].d.z = 0xffffffffu;
+    if (!(left & kLeafBit)) nd[left].d.z = (uint32_t)i;
+    if (!(right & kLeafBit)) nd[right].d.z = (uint32_t)i;
+  }
   if (left & kLeafBit) leaf_parent[left & ~kLeafBit] = (uint32_t)i;
-  else nodes[left].d.z = (uint32_t)i;
   if (right & kLeafBit) leaf_parent[right & ~kLeafBit] = (uint32_t)i;
-  else nodes[right].d.z = (uint32_t)i;
 }
 
 __device__ __forceinline__ void write_slot(Node* node, int slot, const float* lo, const float* hi) {
@@ -95,38 +107,52 @@ __device__ __forceinline__ void read_union(const Node* node, float* lo, float* h
   }
 }
 
-// one thread per leaf: GenRBFBounds (deviceCodeBounds.hlsl:45-81), then walk up the tree; the
-// second child to arrive at an internal node computes its box.
-__global__ void k_refit(const float4* __restrict__ rec0, const float* __restrict__ rgeom, uint64_t n,
-                        uint32_t ppl, uint32_t nleaves, Node* nodes, const uint32_t* __restrict__ leaf_parent,
-                        uint32_t* counters, float* __restrict__ leaf_box, float* __restrict__ root_box) {
-  uint64_t l = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (l >= nleaves) return;
-  const float inf = __int_as_float(0x7f800000);
-  float lo[3] = {inf, inf, inf}, hi[3] = {-inf, -inf, -inf};
-  for (uint32_t k = 0; k < ppl; ++k) {
-    uint64_t i = l * ppl + k;
-    if (i >= n) break;
-    float r = __ldg(rgeom + i);
-    if (r < 0.0f) continue;  // radiusPercent == 0
-    float4 p = __ldg(rec0 + i);
-    lo[0] = fminf(lo[0], p.x - r); lo[1] = fminf(lo[1], p.y - r); lo[2] = fminf(lo[2], p.z - r);
-    hi[0] = fmaxf(hi[0], p.x + r); hi[1] = fmaxf(hi[1], p.y + r); hi[2] = fmaxf(hi[2], p.z + r);
-  }
+__device__ __forceinline__ void nan_if_empty(float* lo, float* hi) {
   if (lo[0] > hi[0] || lo[1] > hi[1] || lo[2] > hi[2]) {
     const float nan = __int_as_float(0x7fc00000);
     lo[0] = lo[1] = lo[2] = hi[0] = hi[1] = hi[2] = nan;
   }
+}
+
+// one thread per leaf: GenRBFBounds (deviceCodeBounds.hlsl:45-81) and the traversal box, then
+// walk up the tree; the second child to arrive at an internal node computes both of its boxes.
+__global__ void k_refit(const float4* __restrict__ rec0, const float* __restrict__ rgeom, uint64_t n,
+                        uint32_t ppl, uint32_t nleaves, Node* nodes, Node* nodes_ref,
+                        const uint32_t* __restrict__ leaf_parent, uint32_t* counters, float* __restrict__ leaf_box,
+                        float* __restrict__ leaf_eff, float* __restrict__ root_box) {
+  uint64_t l = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (l >= nleaves) return;
+  const float inf = __int_as_float(0x7f800000);
+  float lo[3] = {inf, inf, inf}, hi[3] = {-inf, -inf, -inf};     // reference bounds
+  float elo[3] = {inf, inf, inf}, ehi[3] = {-inf, -inf, -inf};   // traversal bounds
+  for (uint32_t k = 0; k < ppl; ++k) {
+    uint64_t i = l * ppl + k;
+    if (i >= n) break;
+    float4 p = __ldg(rec0 + i);
+    float r = __ldg(rgeom + i);
+    if (r >= 0.0f) {  // radiusPercent != 0
+      lo[0] = fminf(lo[0], p.x - r); lo[1] = fminf(lo[1], p.y - r); lo[2] = fminf(lo[2], p.z - r);
+      hi[0] = fmaxf(hi[0], p.x + r); hi[1] = fmaxf(hi[1], p.y + r); hi[2] = fmaxf(hi[2], p.z + r);
+    }
+    if (p.w > 0.0f) {
+      elo[0] = fminf(elo[0], p.x - p.w); elo[1] = fminf(elo[1], p.y - p.w); elo[2] = fminf(elo[2], p.z - p.w);
+      ehi[0] = fmaxf(ehi[0], p.x + p.w); ehi[1] = fmaxf(ehi[1], p.y + p.w); ehi[2] = fmaxf(ehi[2], p.z + p.w);
+    }
+  }
+  nan_if_empty(lo, hi);
+  nan_if_empty(elo, ehi);
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     leaf_box[6 * l + a] = lo[a];
     leaf_box[6 * l + 3 + a] = hi[a];
+    leaf_eff[6 * l + a] = elo[a];
+    leaf_eff[6 * l + 3 + a] = ehi[a];
   }
   if (nleaves == 1) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      root_box[a] = lo[a];
-      root_box[3 + a] = hi[a];
+      root_box[a] = elo[a];
+      root_box[3 + a] = ehi[a];
     }
     return;
   }
@@ -134,18 +160,21 @@ __global__ void k_refit(const float4* __restrict__ rec0, const float* __restrict
   uint32_t parent = leaf_parent[l];
   for (int guard = 0; guard < 256; ++guard) {
     Node* pn = nodes + parent;
+    Node* pr = nodes_ref + parent;
     int slot = (pn->d.x == child) ? 0 : 1;
-    write_slot(pn, slot, lo, hi);
+    write_slot(pn, slot, elo, ehi);
+    write_slot(pr, slot, lo, hi);
     __threadfence();
     if (atomicAdd(counters + parent, 1u) == 0u) return;
     __threadfence();
-    read_union(pn, lo, hi);
+    read_union(pn, elo, ehi);
+    read_union(pr, lo, hi);
     uint32_t up = pn->d.z;
     if (up == 0xffffffffu) {
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        root_box[a] = lo[a];
-        root_box[3 + a] = hi[a];
+        root_box[a] = elo[a];
+        root_box[3 + a] = ehi[a];
       }
       return;
     }
@@ -157,32 +186,32 @@ __global__ void k_refit(const float4* __restrict__ rec0, const float* __restrict
 }  // namespace
 
 cudaError_t launch_prepass(const float4* xyzw, const float* radii, uint64_t n, const float4* tf_color, int nc,
-                           const float* tf_radius, int nr, float rbf_radius, float4* rec0, float4* w4,
-                           float* rgeom, cudaStream_t st) {
+                           const float* tf_radius, int nr, float rbf_radius, float alpha_floor, float4* rec0,
+                           float4* w4, float* rgeom, cudaStream_t st) {
   if (!n) return cudaSuccess;
-  k_prepass<<<blocks_for(n, 256), 256, 0, st>>>(xyzw, radii, n, tf_color, nc, tf_radius, nr, rbf_radius, rec0,
-                                                w4, rgeom);
+  k_prepass<<<blocks_for(n, 256), 256, 0, st>>>(xyzw, radii, n, tf_color, nc, tf_radius, nr, rbf_radius,
+                                                alpha_floor, rec0, w4, rgeom);
   return cudaGetLastError();
 }
 
 cudaError_t launch_karras(const uint64_t* sorted_keys, uint64_t n, uint32_t ppl, uint32_t nleaves, Node* nodes,
-                          uint32_t* leaf_parent, cudaStream_t st) {
+                          Node* nodes_ref, uint32_t* leaf_parent, cudaStream_t st) {
   (void)n;
   if (nleaves < 2) return cudaSuccess;
-  k_karras<<<blocks_for(nleaves - 1, 256), 256, 0, st>>>(sorted_keys, ppl, nleaves, nodes, leaf_parent);
+  k_karras<<<blocks_for(nleaves - 1, 256), 256, 0, st>>>(sorted_keys, ppl, nleaves, nodes, nodes_ref, leaf_parent);
   return cudaGetLastError();
 }
 
 cudaError_t launch_refit(const float4* rec0, const float* rgeom, uint64_t n, uint32_t ppl, uint32_t nleaves,
-                         Node* nodes, const uint32_t* leaf_parent, uint32_t* counters, float* leaf_box,
-                         float* root_box, cudaStream_t st) {
+                         Node* nodes, Node* nodes_ref, const uint32_t* leaf_parent, uint32_t* counters,
+                         float* leaf_box, float* leaf_eff, float* root_box, cudaStream_t st) {
   if (!nleaves) return cudaSuccess;
   if (nleaves > 1) {
     cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(uint32_t) * (nleaves - 1), st);
     if (e != cudaSuccess) return e;
   }
-  k_refit<<<blocks_for(nleaves, 256), 256, 0, st>>>(rec0, rgeom, n, ppl, nleaves, nodes, leaf_parent, counters,
-                                                   leaf_box, root_box);
+  k_refit<<<blocks_for(nleaves, 256), 256, 0, st>>>(rec0, rgeom, n, ppl, nleaves, nodes, nodes_ref, leaf_parent,
+                                                   counters, leaf_box, leaf_eff, root_box);
   return cudaGetLastError();
 }
 

@@ -23,6 +23,14 @@ struct Ray {
   float tmin, tmax;
 };
 
+// count-mode instrumentation: indices into RenderLaunch::counters
+enum { kCtrSteps = 2, kCtrStages = 3, kCtrOverflows = 4, kCtrPointQueries = 5, kCtrCandChecks = 6,
+       kCtrEvals = 7, kCtrStageNodes = 8, kCtrPointNodes = 9 };
+
+__device__ __forceinline__ void ctr_add(unsigned long long* c, int i, unsigned long long v) {
+  if (c) atomicAdd(c + i, v);
+}
+
 struct Sample {
   int count;
   long long a0, a1, a2, a3;
@@ -60,8 +68,10 @@ __device__ __forceinline__ bool inside(float lx, float ly, float lz, float hx, f
 }
 
 // POINT: every leaf whose box contains x, then the exact particle test
-__device__ void point_query(const SceneView& s, float3 x, Sample& acc, uint32_t* status) {
+__device__ void point_query(const SceneView& s, float3 x, Sample& acc, uint32_t* status,
+                            unsigned long long* ctr = nullptr) {
   sample_clear(acc);
+  ctr_add(ctr, kCtrPointQueries, 1);
   if (s.nleaves == 0) return;
   if (!inside(s.root_lo[0], s.root_lo[1], s.root_lo[2], s.root_hi[0], s.root_hi[1], s.root_hi[2], x)) return;
   if (s.root & kLeafBit) {
@@ -71,7 +81,9 @@ __device__ void point_query(const SceneView& s, float3 x, Sample& acc, uint32_t*
   uint32_t stack[kStackSize];
   int sp = 0;
   uint32_t node = s.root;
+  unsigned long long visits = 0;
   while (true) {
+    ++visits;
     const Node* nd = s.nodes + node;
     float4 a = __ldg(&nd->a), b = __ldg(&nd->b), c = __ldg(&nd->c);
     uint2 ch = __ldg(reinterpret_cast<const uint2*>(&nd->d));
@@ -101,6 +113,7 @@ __device__ void point_query(const SceneView& s, float3 x, Sample& acc, uint32_t*
       node = stack[--sp];
     }
   }
+  ctr_add(ctr, kCtrPointNodes, visits);
 }
 
 // slab test of a (slack-inflated) box against the ray segment [t0, t1]
@@ -127,9 +140,11 @@ struct Stager {
   float len_min, len_max;
   float rb_enter, rb_exit;  // ray interval inside the inflated root box
   float3 inv;
+  unsigned long long* ctr;  // count mode only
 
-  __device__ void init(const SceneView& s, const Ray& ray, float unit, char* smem) {
+  __device__ void init(const SceneView& s, const Ray& ray, float unit, char* smem, unsigned long long* counters) {
     const int t = threadIdx.x;
+    ctr = counters;
     idx = reinterpret_cast<uint32_t*>(smem) + t;
     lo = reinterpret_cast<float*>(smem + sizeof(uint32_t) * CAP * kBlock) + t;
     hi = reinterpret_cast<float*>(smem + (sizeof(uint32_t) + sizeof(float)) * CAP * kBlock) + t;
@@ -163,6 +178,7 @@ struct Stager {
   // stage all particles whose inflated sphere meets [t0, t1]; false on buffer overflow
   __device__ bool stage(const SceneView& s, const Ray& ray, float t0, float t1, uint32_t* status) {
     ncand = 0;
+    ctr_add(ctr, kCtrStages, 1);
     const float eps = s.eps;
     uint32_t stack[kStackSize];
     int sp = 0;
@@ -175,6 +191,7 @@ struct Stager {
       if (root_leaf) {
         leaves[nl++] = s.root & ~kLeafBit;
       } else {
+        ctr_add(ctr, kCtrStageNodes, 1);
         const Node* nd = s.nodes + node;
         float4 a = __ldg(&nd->a), b = __ldg(&nd->b), c = __ldg(&nd->c);
         uint2 ch = __ldg(reinterpret_cast<const uint2*>(&nd->d));
@@ -249,6 +266,7 @@ struct Stager {
         len = fminf(len * 2.0f, len_max);
         return;
       }
+      ctr_add(ctr, kCtrOverflows, 1);
       len = len * 0.5f;
       if (len < len_min) break;
     }
@@ -261,15 +279,19 @@ struct Stager {
 
   __device__ __forceinline__ void sample(const SceneView& s, float t, float3 x, Sample& acc, uint32_t* status) {
     if (ncand < 0) {
-      point_query(s, x, acc, status);
+      point_query(s, x, acc, status, ctr);
       return;
     }
     sample_clear(acc);
+    unsigned long long ev = 0;
     for (int j = 0; j < ncand; ++j) {
       float a = lo[j * kBlock], b = hi[j * kBlock];
       if (t < a || t > b) continue;
+      ++ev;
       eval_particle(s, idx[j * kBlock], x, acc);
     }
+    ctr_add(ctr, kCtrCandChecks, (unsigned long long)ncand);
+    ctr_add(ctr, kCtrEvals, ev);
   }
 };
 
@@ -369,7 +391,7 @@ template <int CAP>
 __device__ __forceinline__ void do_sample(const RenderLaunch& L, Stager<CAP>& st, const Ray& ray, float t, float3 x,
                                           Sample& acc) {
   if (L.traversal == AARBF_TRAVERSAL_POINT) {
-    point_query(L.s, x, acc, L.status);
+    point_query(L.s, x, acc, L.status, L.counters);
   } else {
     st.cover(L.s, ray, t, L.status);
     st.sample(L.s, t, x, acc, L.status);
@@ -380,7 +402,7 @@ __device__ __forceinline__ void do_sample(const RenderLaunch& L, Stager<CAP>& st
 template <int CAP>
 __device__ void track_delta(const RenderLaunch& L, Tracker& tr, const Ray& ray, bool from_entry, char* smem) {
   Stager<CAP> st;
-  st.init(L.s, ray, L.unit, smem);
+  st.init(L.s, ray, L.unit, smem, L.counters);
   if (!from_entry) tr.t = ray.tmin;
   for (; tr.i < kMaxDepth; ++tr.i) {
     float u = lcg_f(tr.rng);
@@ -405,7 +427,7 @@ __device__ void track_delta(const RenderLaunch& L, Tracker& tr, const Ray& ray, 
 template <int CAP>
 __device__ void track_march(const RenderLaunch& L, Tracker& tr, const Ray& ray, char* smem) {
   Stager<CAP> st;
-  st.init(L.s, ray, L.unit, smem);
+  st.init(L.s, ray, L.unit, smem, L.counters);
   float rhs = -dlog(1.0f - tr.random * 0.99f);
   for (; tr.i < kMaxDepth; ++tr.i) {
     tr.t = tr.t + L.unit;
@@ -432,11 +454,224 @@ __device__ void track_march(const RenderLaunch& L, Tracker& tr, const Ray& ray, 
   }
 }
 
+// ---- delta tracking with per-bin majorants (native mode) -----------------------------------
+// Bins [t0 + k L, t0 + (k+1) L) along the ray. Majorant of a bin = density_scale (1 + 2^-7) times
+// the exact fixed-point sum over particles whose sphere meets the bin's segment of a^3 rho at
+// their closest approach to the segment. The staged candidates of a run of bins serve both the
+// majorants and the density at tentative collisions; runs of empty bins are skipped without
+// drawing random numbers, which leaves the sample stream unchanged.
+
+// a bin is split in halves while majorant * length (its expected number of tentative steps)
+// exceeds kSplitSteps, at most kSplitDepth times: tight majorants across steep density gradients
+constexpr float kSplitSteps = 4.0f;
+constexpr int kSplitDepth = 10;
+
+// a^3 rho at particle i's closest approach to [b0, b1]; 0 when its sphere misses the segment
+__device__ __forceinline__ float bin_contrib(const SceneView& s, const Ray& ray, uint32_t i, float b0, float b1) {
+  float4 r = __ldg(s.rec0 + i);
+  float vx = r.x - ray.o.x, vy = r.y - ray.o.y, vz = r.z - ray.o.z;
+  float tc = (vx * ray.d.x + vy * ray.d.y) + vz * ray.d.z;
+  float wx = vx - tc * ray.d.x, wy = vy - tc * ray.d.y, wz = vz - tc * ray.d.z;
+  float h2 = (wx * wx + wy * wy) + wz * wz;
+  float tcl = fminf(fmaxf(tc, b0), b1);
+  float dt = tcl - tc;
+  float d2 = h2 + dt * dt;
+  float r2 = r.w * r.w;
+  if (!(d2 < r2)) return 0.0f;
+  float q2 = (9.0f * d2) / r2;
+  return dexp(-0.5f * q2) * __ldg(&s.w4[i].x);
+}
+
+// majorant sum of one bin without a buffer: every particle of every leaf whose inflated box
+// meets the bin (used when a single bin holds more candidates than the staging buffer)
+__device__ long long bin_sum_direct(const SceneView& s, const Ray& ray, float3 inv, float b0, float b1,
+                                    uint32_t* status, unsigned long long* ctr) {
+  long long acc = 0;
+  if (s.nleaves == 0) return 0;
+  uint32_t stack[kStackSize];
+  int sp = 0;
+  uint32_t node = s.root;
+  const bool root_leaf = (s.root & kLeafBit) != 0;
+  while (true) {
+    uint32_t leaves[2];
+    int nl = 0;
+    uint32_t n0 = 0xffffffffu, n1 = 0xffffffffu;
+    if (root_leaf) {
+      leaves[nl++] = s.root & ~kLeafBit;
+    } else {
+      ctr_add(ctr, kCtrStageNodes, 1);
+      const Node* nd = s.nodes + node;
+      float4 a = __ldg(&nd->a), b = __ldg(&nd->b), c = __ldg(&nd->c);
+      uint2 ch = __ldg(reinterpret_cast<const uint2*>(&nd->d));
+      if (seg_box(a.x, a.y, a.z, a.w, b.x, b.y, ray.o, inv, b0, b1, s.eps)) {
+        if (ch.x & kLeafBit) leaves[nl++] = ch.x & ~kLeafBit;
+        else n0 = ch.x;
+      }
+      if (seg_box(b.z, b.w, c.x, c.y, c.z, c.w, ray.o, inv, b0, b1, s.eps)) {
+        if (ch.y & kLeafBit) leaves[nl++] = ch.y & ~kLeafBit;
+        else n1 = ch.y;
+      }
+    }
+    for (int k = 0; k < nl; ++k) {
+      uint64_t e0 = (uint64_t)leaves[k] * s.ppl + s.ppl;
+      if (e0 > s.n) e0 = s.n;
+      for (uint64_t i = (uint64_t)leaves[k] * s.ppl; i < e0; ++i) acc += fix40(bin_contrib(s, ray, (uint32_t)i, b0, b1));
+    }
+    if (root_leaf) break;
+    if (n0 != 0xffffffffu && n1 != 0xffffffffu) {
+      if (sp == kStackSize) {
+        atomicOr(status, kStatusStackOverflow);
+        break;
+      }
+      stack[sp++] = n1;
+      node = n0;
+    } else if (n0 != 0xffffffffu) {
+      node = n0;
+    } else if (n1 != 0xffffffffu) {
+      node = n1;
+    } else {
+      if (sp == 0) break;
+      node = stack[--sp];
+    }
+  }
+  return acc;
+}
+
+template <int CAP>
+__device__ void track_majorant(const RenderLaunch& L, Tracker& tr, const Ray& ray, char* smem) {
+  Stager<CAP> st;
+  st.init(L.s, ray, L.unit, smem, L.counters);
+  const float Lb = L.bin_length;
+  const float scale = L.density_scale;
+  const float minf = scale * 1.0078125f;
+  const float t0 = tr.t;
+  int k = 0;
+  float t = t0;
+  int seg_end = 0;   // bins below seg_end are covered by the staged candidates
+  int nb = 16;       // bins per staging
+  bool direct = false;
+  for (int guard = 0; guard < (1 << 26); ++guard) {
+    float b0 = t0 + (float)k * Lb;
+    float b1 = t0 + (float)(k + 1) * Lb;
+    if (!(b0 < ray.tmax) || !(b1 > b0)) break;
+    if (k >= seg_end) {
+      // bins ending before the scene's root box are empty
+      if (b1 < st.rb_enter) {
+        int ks = (int)floorf((st.rb_enter - t0) / Lb) - 1;
+        if (ks > k) {
+          k = ks;
+          t = t0 + (float)k * Lb;
+          continue;
+        }
+      }
+      if (b0 > st.rb_exit) break;  // nothing further along the ray
+      direct = false;
+      for (;;) {
+        float te = t0 + (float)(k + nb) * Lb;
+        if (st.stage(L.s, ray, b0, te, L.status)) {
+          seg_end = k + nb;
+          if (nb < 64) nb *= 2;
+          break;
+        }
+        ctr_add(L.counters, kCtrOverflows, 1);
+        nb >>= 1;
+        if (nb == 0) {
+          direct = true;
+          seg_end = k + 1;
+          nb = 1;
+          break;
+        }
+      }
+      if (!direct) {
+        if (st.ncand == 0) {  // the whole staged run is empty
+          k = seg_end;
+          t = t0 + (float)k * Lb;
+          continue;
+        }
+        float lo_min = __int_as_float(0x7f800000);
+        for (int j = 0; j < st.ncand; ++j) lo_min = fminf(lo_min, st.lo[j * kBlock]);
+        int ks = (int)floorf((lo_min - t0) / Lb) - 1;
+        if (ks > k && ks < seg_end) {
+          k = ks;
+          t = t0 + (float)k * Lb;
+          continue;
+        }
+      }
+    }
+    // [b0, b1), split in halves (front first) while majorant * length > kSplitSteps
+    float lo = b0, hi = b1;
+    int depth = 0, np = 0;
+    float pend_hi[kSplitDepth];
+    int pend_depth[kSplitDepth];
+    for (;;) {
+      long long acc = 0;
+      if (direct) {
+        acc = bin_sum_direct(L.s, ray, st.inv, lo, hi, L.status, L.counters);
+      } else {
+        for (int j = 0; j < st.ncand; ++j) {
+          if (st.hi[j * kBlock] < lo || st.lo[j * kBlock] > hi) continue;
+          acc += fix40(bin_contrib(L.s, ray, st.idx[j * kBlock], lo, hi));
+        }
+      }
+      float M = ((float)acc * kFixInv) * minf;
+      if (M > 0.0f) {
+        float mid = lo + 0.5f * (hi - lo);
+        if (M * (hi - lo) > kSplitSteps && depth < kSplitDepth && mid > lo && mid < hi) {
+          pend_hi[np] = hi;
+          pend_depth[np] = depth + 1;
+          ++np;
+          hi = mid;
+          depth += 1;
+          continue;
+        }
+        t = lo;
+        for (;;) {
+          if (tr.i >= kMaxDepth) {
+            tr.t = t;
+            return;
+          }
+          tr.i += 1;
+          float u = lcg_f(tr.rng);
+          float step = -dlog(1.0f - u) / M;
+          t = t + step;
+          if (t >= hi || t >= ray.tmax) break;
+          float3 x = make_float3(ray.o.x + t * ray.d.x, ray.o.y + t * ray.d.y, ray.o.z + t * ray.d.z);
+          Sample smp;
+          if (direct) {
+            point_query(L.s, x, smp, L.status, L.counters);
+          } else {
+            st.sample(L.s, t, x, smp, L.status);
+          }
+          float D = (float)smp.a0 * kFixInv;
+          float sigma = D * scale;
+          if (lcg_f(tr.rng) < sigma / M) {
+            float3 c = sample_color(L, smp, D);
+            tr.albedo = make_float4(c.x, c.y, c.z, 1.0f);
+            tr.t = t;
+            return;
+          }
+        }
+      }
+      if (np == 0) break;
+      lo = hi;
+      --np;
+      hi = pend_hi[np];
+      depth = pend_depth[np];
+    }
+    k += 1;
+    t = b1;
+  }
+  tr.t = t;
+}
+
 template <int CAP>
 __device__ __forceinline__ void track(const RenderLaunch& L, Tracker& tr, const Ray& ray, bool from_entry,
                                       char* smem) {
+  const int i0 = tr.i;
   if (tr.marching) track_march<CAP>(L, tr, ray, smem);
+  else if (L.flags & kFlagMajorantTracking) track_majorant<CAP>(L, tr, ray, smem);
   else track_delta<CAP>(L, tr, ray, from_entry, smem);
+  ctr_add(L.counters, kCtrSteps, (unsigned long long)(tr.i - i0 + 1));
 }
 
 // ParticleRBFRayGen body for one sample (deviceCodeRBF.hlsl:206-324)
@@ -523,45 +758,68 @@ __device__ float4 raygen_sample(const RenderLaunch& L, uint32_t frame, int px, i
   return over4(color, make_float4(0.0f, 0.0f, 0.0f, 1.0f));
 }
 
+// Persistent kernel: each thread repeatedly takes the next pixel from a global counter (32
+// consecutive items form an 8x4 pixel tile) and renders all of its samples, so long rays no
+// longer hold up the rest of a statically assigned tile.
 template <int CAP>
 __global__ void __launch_bounds__(kBlock) k_render(const RenderLaunch L) {
   extern __shared__ __align__(16) char smem[];
-  const int px = blockIdx.x * 16 + (threadIdx.x & 15);
-  const int py = blockIdx.y * 8 + (threadIdx.x >> 4);
-  if (px >= L.width || py >= L.height) return;
-  const size_t ofs = (size_t)px + (size_t)L.width * (size_t)py;
-  float4 prev = L.accum[ofs];
-  float4 fin = prev;
-  float noise = 0.0f;
+  const uint32_t tiles_x = (uint32_t)(L.width + 7) / 8u;
+  const uint32_t total = tiles_x * ((uint32_t)(L.height + 3) / 4u) * 32u;
   const uint32_t spp = L.spp ? L.spp : 1u;
-  for (uint32_t k = 0; k < spp; ++k) {
-    uint32_t frame = (L.frame_id + k) & 0xffffu;
-    uint32_t aid = (L.accum_id + k) & 0xffffu;
-    float4 c = raygen_sample<CAP>(L, frame, px, py, noise, smem);
-    // running mean, deviceCodeRBF.hlsl:326-328
-    float fa = (float)aid;
-    float wa = 1.0f / fa, wb = (float)((int)aid - 1) / fa;
-    fin.x = wa * c.x + wb * prev.x;
-    fin.y = wa * c.y + wb * prev.y;
-    fin.z = wa * c.z + wb * prev.z;
-    fin.w = wa * c.w + wb * prev.w;
-    prev = fin;
+  for (;;) {
+    uint32_t item = atomicAdd(L.work_counter, 1u);
+    if (item >= total) break;
+    uint32_t tile = item >> 5, in = item & 31u;
+    const int px = (int)((tile % tiles_x) * 8u + (in & 7u));
+    const int py = (int)((tile / tiles_x) * 4u + (in >> 3));
+    if (px >= L.width || py >= L.height) continue;
+    const size_t ofs = (size_t)px + (size_t)L.width * (size_t)py;
+    float4 prev = L.accum[ofs];
+    float4 fin = prev;
+    float noise = 0.0f;
+    const bool cost = (L.flags & kFlagCostImage) != 0;
+    const long long c0 = cost ? clock64() : 0;
+    for (uint32_t k = 0; k < spp; ++k) {
+      uint32_t frame = (L.frame_id + k) & 0xffffu;
+      uint32_t aid = (L.accum_id + k) & 0xffffu;
+      float4 c = raygen_sample<CAP>(L, frame, px, py, noise, smem);
+      // running mean, deviceCodeRBF.hlsl:326-328
+      float fa = (float)aid;
+      float wa = 1.0f / fa, wb = (float)((int)aid - 1) / fa;
+      fin.x = wa * c.x + wb * prev.x;
+      fin.y = wa * c.y + wb * prev.y;
+      fin.z = wa * c.z + wb * prev.z;
+      fin.w = wa * c.w + wb * prev.w;
+      prev = fin;
+    }
+    L.accum[ofs] = fin;
+    if (L.flags & kFlagShowNoise) fin = make_float4(noise, noise, noise, 1.0f);
+    // diagnostic: the image's alpha channel receives the pixel's cost in SM clock cycles
+    if (cost) fin.w = (float)(clock64() - c0);
+    L.image[ofs] = fin;
   }
-  L.accum[ofs] = fin;
-  if (L.flags & kFlagShowNoise) fin = make_float4(noise, noise, noise, 1.0f);
-  L.image[ofs] = fin;
 }
 
 template <int CAP>
 cudaError_t launch_cap(const RenderLaunch& L, cudaStream_t st) {
-  size_t smem = (sizeof(uint32_t) + 2 * sizeof(float)) * CAP * kBlock;
-  static bool configured = false;
-  if (!configured) {
+  const size_t smem = (sizeof(uint32_t) + 2 * sizeof(float)) * CAP * kBlock;
+  static int blocks = 0;
+  if (!blocks) {
     cudaError_t e = cudaFuncSetAttribute(k_render<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    configured = true;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render<CAP>, kBlock, smem);
+    if (e != cudaSuccess) return e;
+    blocks = sms * (per_sm > 0 ? per_sm : 1);
   }
-  dim3 grid((L.width + 15) / 16, (L.height + 7) / 8);
+  cudaError_t e = cudaMemsetAsync(L.work_counter, 0, sizeof(uint32_t), st);
+  if (e != cudaSuccess) return e;
+  uint32_t tiles = (uint32_t)((L.width + 7) / 8) * (uint32_t)((L.height + 3) / 4);
+  int grid = (int)(tiles * 32u + kBlock - 1) / kBlock;
+  if (grid > blocks) grid = blocks;
   k_render<CAP><<<grid, kBlock, smem, st>>>(L);
   return cudaGetLastError();
 }
@@ -570,7 +828,12 @@ cudaError_t launch_cap(const RenderLaunch& L, cudaStream_t st) {
 
 cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st) {
   if (L.width <= 0 || L.height <= 0) return cudaSuccess;
-  return launch_cap<32>(L, st);
+  switch (L.candidate_cap) {
+    case 16: return launch_cap<16>(L, st);
+    case 64: return launch_cap<64>(L, st);
+    case 128: return launch_cap<128>(L, st);
+    default: return launch_cap<32>(L, st);
+  }
 }
 
 }  // namespace aarbf

@@ -66,7 +66,7 @@ __device__ bool traverse(const RenderLaunch& L, float3 o, float3 inv, float t0, 
     if (root_leaf) {
       leaves[nl++] = s.root & ~kLeafBit;
     } else {
-      const Node* nd = s.nodes + node;
+      const Node* nd = s.nodes_ref + node;  // reference bounds: splatting ignores opacity
       float4 a = __ldg(&nd->a), b = __ldg(&nd->b), c = __ldg(&nd->c);
       uint2 ch = __ldg(reinterpret_cast<const uint2*>(&nd->d));
       if (seg_box(a.x, a.y, a.z, a.w, b.x, b.y, o, inv, t0, t1, pad)) {

@@ -55,7 +55,14 @@ def parse():
     ap.add_argument("--unit", type=float, default=0.001)
     ap.add_argument("--density-scale", type=float, default=50.0)
     ap.add_argument("--traversal", type=int, default=0, help="0 staged, 1 point query")
-    ap.add_argument("--ppl", type=int, default=1)
+    ap.add_argument("--ppl", type=int, default=8, help="particles per BVH leaf")
+    ap.add_argument("--estimator", default="majorant", choices=["majorant", "plain"],
+                    help="delta tracking with per-bin majorants, or with the global majorant 1/unit")
+    ap.add_argument("--bin", type=float, default=16.0, help="majorant bin length in units")
+    ap.add_argument("--alpha-floor", type=float, default=1.0 / 255.0,
+                    help="opacity below this is transparent (1/255: the 8-bit transfer-function resolution)")
+    ap.add_argument("--cap", type=int, default=32, help="staged candidates per ray (16/32/64/128)")
+    ap.add_argument("--plain-spp", type=int, default=1, help="spp of the plain-estimator comparison (0: skip)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
@@ -154,16 +161,20 @@ def domain_of(xyzw):
     return d
 
 
-def params_for(args, dom, rmax, frame_id=0):
+def params_for(args, dom, rmax, frame_id=0, estimator=None, spp=None):
     from aarbf import scenes
-    return scenes.native_params(scenes.orbit_camera(), args.width, args.height, rmax, args.unit,
-                                args.density_scale, dom, spp=args.spp, frame_id=frame_id,
-                                traversal=args.traversal)
+    est = estimator or args.estimator
+    rp = scenes.native_params(scenes.orbit_camera(), args.width, args.height, rmax, args.unit,
+                              args.density_scale, dom, spp=spp or args.spp, frame_id=frame_id,
+                              traversal=args.traversal, majorant=(est == "majorant"),
+                              bin_length=args.bin * args.unit)
+    rp.candidate_cap = args.cap
+    return rp
 
 
 def cpu_scene(args, sc, tf, dom, rbf_radius):
     import oracle.oracle as orc
-    return orc.build_scene(sc.xyzw, sc.radii, dom, args.ppl, rbf_radius, tf)[0]
+    return orc.build_scene(sc.xyzw, sc.radii, dom, args.ppl, rbf_radius, tf, args.alpha_floor)[0]
 
 
 def cpu_sample(args, scene, rp, target_s, threads):
@@ -229,8 +240,12 @@ def run_reference(args):
 def config_dict(args):
     return {"workload": f"clusters_{args.particles // 1_000_000}M_{args.width}x{args.height}_{args.spp}spp_delta_tracking",
             "particles": args.particles, "width": args.width, "height": args.height, "spp": args.spp,
-            "estimator": "delta tracking + shadow ray", "unit": args.unit, "density_scale": args.density_scale,
+            "estimator": ("delta tracking with per-bin majorants (bin %g units) + shadow ray" % args.bin
+                          if args.estimator == "majorant" else
+                          "delta tracking with the global majorant 1/unit + shadow ray"),
+            "unit": args.unit, "density_scale": args.density_scale,
             "traversal": "staged" if args.traversal == 0 else "point", "particles_per_leaf": args.ppl,
+            "alpha_floor": args.alpha_floor, "candidate_cap": args.cap,
             "l2": "inputs_larger_than_l2", "parallelism": f"replicas{args.gpus}"}
 
 
@@ -259,6 +274,7 @@ def main():
     radii_pin = torch.from_numpy(sc.radii).pin_memory()
     ctx.set_domain(dom)
     ctx.set_transfer_functions_f32(*tf)
+    ctx.set_opacity_floor(args.alpha_floor)
     ctx.set_particles(xyzw_pin, radii_pin, stream=sp)
     t_b0 = time.perf_counter()
     ctx.build(rmax, args.ppl, stream=sp)
@@ -300,11 +316,27 @@ def main():
 
     # roofline accounting: one counted launch (untimed)
     rp = params_for(args, dom, rmax, frame_id=0)
-    parts, visits = ctx.render_count(rp, W, H, accum, image, stream=sp)
+    counts = ctx.render_count(rp, W, H, accum, image, stream=sp)
+    parts, visits = counts["segment_particles"], counts["segment_nodes"]
     alg_bytes = 20 * parts + 64 * visits + 48 * W * H
     launch_s = t / args.steps
     achieved = alg_bytes / launch_s / 1e9
     peak, peak_kind = measured_peak()
+
+    # the plain estimator (global majorant 1/unit, the reference's tracking loop) on the same frame
+    plain = None
+    if args.plain_spp > 0 and args.estimator == "majorant":
+        rpp = params_for(args, dom, rmax, frame_id=0, estimator="plain", spp=args.plain_spp)
+        ctx.render(rpp, W, H, accum, image, stream=sp)
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        ctx.render(rpp, W, H, accum, image, stream=sp)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        tp = g0.elapsed_time(g1) / 1e3
+        plain = {"value": W * H * args.plain_spp / tp / 1e6, "unit": UNIT, "spp": args.plain_spp,
+                 "ms": tp * 1e3}
 
     # end to end through the C ABI with host buffers
     e2e = None
@@ -351,9 +383,9 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profiled_traffic(), "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes, "particles_on_segments": parts,
-                         "node_visits": visits},
+                         "node_visits": visits, "kernel_counters": counts},
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": args.steps,
-            "build_ms": build_s * 1e3,
+            "build_ms": build_s * 1e3, "plain_estimator": plain,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

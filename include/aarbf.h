@@ -50,7 +50,11 @@ enum {
   AARBF_FLAG_VISUALIZE_ATTRIBUTES = 1u << 2, /* visualizeAttributes (reference default: on) */
   AARBF_FLAG_TRACK_FROM_ENTRY = 1u << 3,     /* native: delta tracking starts at tenter + unit*xi */
   AARBF_FLAG_DENSITY_LINEAR = 1u << 4,       /* native: density = min(D * density_gain, 1) */
-  AARBF_FLAG_SPLAT_PARTICLE_RADIUS = 1u << 5 /* native: splats use the per-particle radius */
+  AARBF_FLAG_SPLAT_PARTICLE_RADIUS = 1u << 5, /* native: splats use the per-particle radius */
+  AARBF_FLAG_MAJORANT_TRACKING = 1u << 6,     /* native: delta tracking with per-bin majorants
+                                                 (extinction = density_scale * D, unclamped) */
+  AARBF_FLAG_COST_IMAGE = 1u << 7             /* diagnostic: image alpha = SM clock cycles the
+                                                 pixel's samples took */
 };
 
 /* Traversal strategies of the render kernel (identical results). */
@@ -79,7 +83,10 @@ typedef struct aarbf_params {
   float density_gain; /* AARBF_FLAG_DENSITY_LINEAR: density scale * unit */
   float jitter_x, jitter_y; /* sub-pixel camera jitter in pixels (0 = reference) */
   int32_t traversal;        /* AARBF_TRAVERSAL_* */
-  int32_t reserved[3];
+  float density_scale;      /* AARBF_FLAG_MAJORANT_TRACKING: extinction per unit length per unit D */
+  float bin_length;         /* AARBF_FLAG_MAJORANT_TRACKING: majorant bin length along a ray */
+  int32_t candidate_cap;    /* staged candidates per ray: 16, 32, 64 or 128 (0 = 32); tuning only,
+                               results are identical for every value */
 } aarbf_params;
 
 /* ---- context -------------------------------------------------------------------------- */
@@ -121,6 +128,11 @@ aarbf_status aarbf_set_transfer_functions_rgba8(aarbf_ctx *ctx, const uint8_t *c
 aarbf_status aarbf_set_transfer_functions_f32(aarbf_ctx *ctx, const float *colormap, int nc,
                                               const float *radiusmap, int nr,
                                               const float *densitymap, int nd);
+/* Opacity below alpha_floor counts as transparent, as opacity 0 does in the any-hit program
+ * (deviceCodeRBF.hlsl:369-372). Default 0 (the reference). With fp32 transfer functions, 1/255
+ * reproduces the resolution of the reference's 8-bit textures. Takes effect at the next
+ * aarbf_build / aarbf_refit. */
+aarbf_status aarbf_set_opacity_floor(aarbf_ctx *ctx, float alpha_floor);
 /* Gradient marks -> 64-entry RGBA8 texture as hostCode.cpp:528-542 (gamma 1/2.2 on rgb when
  * gamma != 0) and :544-572 (grey maps). marks: npos positions + npos RGBA colours. */
 aarbf_status aarbf_marks_to_rgba8(const float *pos, const float *rgba, int nmarks, int gamma,
@@ -143,9 +155,13 @@ aarbf_status aarbf_refit(aarbf_ctx *ctx, float rbf_radius, void *stream);
  * accum is read-modify-written (running mean over accum_id), image receives the frame. */
 aarbf_status aarbf_render(aarbf_ctx *ctx, const aarbf_params *p, int width, int height,
                           float *accum, float *image, void *stream);
-/* aarbf_render plus accounting (no counterpart in the reference; for roofline figures):
- * counts[0] = particles whose sphere meets a traversed ray segment (primary [start, termination]
- * and shadow), counts[1] = BVH nodes those segment queries visit. Synchronises `stream`. */
+/* aarbf_render plus accounting (no counterpart in the reference; for roofline figures).
+ * counts has AARBF_COUNT_SLOTS entries: [0] particles whose sphere meets a traversed ray segment
+ * (primary [start, termination] and shadow), [1] BVH nodes those segment queries visit, then the
+ * kernel's own work: [2] tracking steps, [3] segment stagings, [4] staging overflows, [5] point
+ * queries, [6] staged-candidate checks, [7] particle evaluations, [8] node visits while staging,
+ * [9] node visits of point queries. Synchronises `stream`. */
+#define AARBF_COUNT_SLOTS 10
 aarbf_status aarbf_render_count(aarbf_ctx *ctx, const aarbf_params *p, int width, int height,
                                 float *accum, float *image, uint64_t *counts, void *stream);
 /* ParticleSplatRayGen (deviceCodeSplat.hlsl:58-193); writes image only. */
@@ -203,10 +219,12 @@ aarbf_status aarbf_get_hilbert_keys(aarbf_ctx *ctx, uint64_t *keys, uint32_t *pe
 aarbf_status aarbf_get_sorted_particles(aarbf_ctx *ctx, float *xyzw);
 /* prepass records: rec0 = (x,y,z,r_eval) x n, w4 = (a^3, pow(rgb,2.2) a^3) x n, rgeom x n */
 aarbf_status aarbf_get_prepass(aarbf_ctx *ctx, float *rec0, float *w4, float *rgeom);
-/* BVH: child codes (bit31 = leaf) of the L-1 internal nodes, their boxes (6 floats each:
- * lo xyz, hi xyz), leaf boxes (6 x L) and the root box (6) */
+/* BVH: child codes (bit31 = leaf) of the L-1 internal nodes, their traversal boxes (6 floats
+ * each: lo xyz, hi xyz), the leaf boxes of the reference's bounds program (6 x L,
+ * GenRBFBounds), the traversal leaf boxes (6 x L, particles that can be hit) and the root
+ * traversal box (6) */
 aarbf_status aarbf_get_bvh(aarbf_ctx *ctx, uint32_t *left, uint32_t *right, float *node_box,
-                           float *leaf_box, float *root_box);
+                           float *leaf_box, float *leaf_eff, float *root_box);
 
 #ifdef __cplusplus
 }

@@ -412,9 +412,10 @@ struct orc_scene {
   float *w4;       /* 4n: alpha^3, pow(r,2.2) a^3, pow(g,2.2) a^3, pow(b,2.2) a^3 */
   float *rgeom;    /* n: bounds radius, -1 when radiusmap == 0 (skipped by the bounds program) */
   uint64_t *leaf_key;
-  float *leaf_box; /* 6 per leaf */
+  float *leaf_box; /* 6 per leaf: the reference's bounds program (radius from radiusmap) */
+  float *leaf_eff; /* 6 per leaf: traversal box from r_eval (particles that can be hit) */
   uint32_t *left, *right;
-  float *node_box; /* 6 per internal node */
+  float *node_box; /* 6 per internal node (union of leaf_eff) */
   float root_box[6];
   uint32_t root;   /* child code of the root */
   /* transfer functions for rendering */
@@ -443,7 +444,7 @@ static void prepass(orc_scene *s, const float *radii, const orc_tf_desc *tf) {
     s->rec0[4 * i + 1] = p[1];
     s->rec0[4 * i + 2] = p[2];
     float a = col[3];
-    if (a == 0.0f) {
+    if (a == 0.0f || a < tf->alpha_floor) { /* transparent: ignored by the any-hit program */
       s->rec0[4 * i + 3] = 0.0f;
       s->w4[4 * i + 0] = s->w4[4 * i + 1] = s->w4[4 * i + 2] = s->w4[4 * i + 3] = 0.0f;
     } else {
@@ -473,6 +474,24 @@ static void leaf_bounds(orc_scene *s) {
     for (int a = 0; a < 3; ++a) {
       s->leaf_box[6 * l + a] = empty ? NAN : lo[a];
       s->leaf_box[6 * l + 3 + a] = empty ? NAN : hi[a];
+    }
+    /* traversal box: the particles that can be hit, p +- r_eval */
+    float el[3] = {INFINITY, INFINITY, INFINITY}, eh[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t k = 0; k < s->ppl; ++k) {
+      uint64_t i = (uint64_t)l * s->ppl + k;
+      if (i >= s->n) break;
+      float r = s->rec0[4 * i + 3];
+      if (!(r > 0.0f)) continue;
+      for (int a = 0; a < 3; ++a) {
+        float c = s->rec0[4 * i + a];
+        el[a] = orc_minf(el[a], c - r);
+        eh[a] = orc_maxf(eh[a], c + r);
+      }
+    }
+    empty = (el[0] > eh[0]) || (el[1] > eh[1]) || (el[2] > eh[2]);
+    for (int a = 0; a < 3; ++a) {
+      s->leaf_eff[6 * l + a] = empty ? NAN : el[a];
+      s->leaf_eff[6 * l + 3 + a] = empty ? NAN : eh[a];
     }
   }
 }
@@ -511,7 +530,7 @@ static void karras(orc_scene *s) {
 }
 
 static const float *child_box(const orc_scene *s, uint32_t c) {
-  return (c & ORC_LEAF_BIT) ? s->leaf_box + 6 * (c & ~ORC_LEAF_BIT) : s->node_box + 6 * c;
+  return (c & ORC_LEAF_BIT) ? s->leaf_eff + 6 * (c & ~ORC_LEAF_BIT) : s->node_box + 6 * c;
 }
 
 static void refit_node(orc_scene *s, uint32_t node) {
@@ -554,6 +573,7 @@ orc_scene *orc_scene_create(const float *xyzw, const float *radii, const uint64_
   s->rgeom = (float *)calloc(nn, sizeof(float));
   s->leaf_key = (uint64_t *)calloc(nl, sizeof(uint64_t));
   s->leaf_box = (float *)calloc(6 * nl, sizeof(float));
+  s->leaf_eff = (float *)calloc(6 * nl, sizeof(float));
   s->left = (uint32_t *)calloc(nl, sizeof(uint32_t));
   s->right = (uint32_t *)calloc(nl, sizeof(uint32_t));
   s->node_box = (float *)calloc(6 * nl, sizeof(float));
@@ -569,7 +589,7 @@ orc_scene *orc_scene_create(const float *xyzw, const float *radii, const uint64_
     s->root = ORC_LEAF_BIT; /* unused */
   } else if (s->nleaves == 1) {
     s->root = 0 | ORC_LEAF_BIT;
-    memcpy(s->root_box, s->leaf_box, 6 * sizeof(float));
+    memcpy(s->root_box, s->leaf_eff, 6 * sizeof(float));
   } else {
     karras(s);
     refit_node(s, 0);
@@ -582,7 +602,8 @@ orc_scene *orc_scene_create(const float *xyzw, const float *radii, const uint64_
 void orc_scene_destroy(orc_scene *s) {
   if (!s) return;
   free(s->xyzw); free(s->rec0); free(s->w4); free(s->rgeom);
-  free(s->leaf_key); free(s->leaf_box); free(s->left); free(s->right); free(s->node_box);
+  free(s->leaf_key); free(s->leaf_box); free(s->leaf_eff); free(s->left); free(s->right);
+  free(s->node_box);
   free(s->color); free(s->density);
   free(s);
 }
@@ -590,12 +611,13 @@ void orc_scene_destroy(orc_scene *s) {
 uint32_t orc_scene_num_leaves(const orc_scene *s) { return s->nleaves; }
 
 void orc_scene_get_bvh(const orc_scene *s, uint32_t *left, uint32_t *right, float *node_box,
-                       float *leaf_box, float *root_box) {
+                       float *leaf_box, float *leaf_eff, float *root_box) {
   uint32_t ni = s->nleaves > 0 ? s->nleaves - 1 : 0;
   if (left) memcpy(left, s->left, ni * sizeof(uint32_t));
   if (right) memcpy(right, s->right, ni * sizeof(uint32_t));
   if (node_box) memcpy(node_box, s->node_box, 6 * (size_t)ni * sizeof(float));
   if (leaf_box) memcpy(leaf_box, s->leaf_box, 6 * (size_t)s->nleaves * sizeof(float));
+  if (leaf_eff) memcpy(leaf_eff, s->leaf_eff, 6 * (size_t)s->nleaves * sizeof(float));
   if (root_box) memcpy(root_box, s->root_box, 6 * sizeof(float));
 }
 
@@ -805,9 +827,194 @@ static void track_march(const orc_scene *s, const orc_params *p, orc_tracker *tr
   }
 }
 
+/* ---- delta tracking with per-bin majorants (native mode; no counterpart in the reference) ----
+ * The ray from its start t0 is cut into bins [t0 + k L, t0 + (k+1) L). The majorant of a bin is
+ * density_scale * (1 + 2^-7) * sum over particles whose sphere meets the bin's segment of
+ * a^3 * rho at the particle's closest approach to the segment (fixed-point sum). Delta tracking
+ * then runs bin by bin: empty bins are crossed without drawing, a tentative step beyond the bin
+ * restarts at the bin boundary (memoryless), a tentative collision at t is real with probability
+ * density_scale * D(t) / majorant. */
+
+typedef struct {
+  uint32_t *idx;
+  size_t n, cap;
+} orc_cands;
+
+static void cands_push(orc_cands *c, uint32_t i) {
+  if (c->n == c->cap) {
+    c->cap = c->cap ? 2 * c->cap : 256;
+    c->idx = (uint32_t *)realloc(c->idx, c->cap * sizeof(uint32_t));
+  }
+  c->idx[c->n++] = i;
+}
+
+static int seg_box_hit(const float *b, const orc_ray *r, const float *inv, float t0, float t1, float e) {
+  float ax = (b[0] - e - r->o[0]) * inv[0], bx = (b[3] + e - r->o[0]) * inv[0];
+  float ay = (b[1] - e - r->o[1]) * inv[1], by = (b[4] + e - r->o[1]) * inv[1];
+  float az = (b[2] - e - r->o[2]) * inv[2], bz = (b[5] + e - r->o[2]) * inv[2];
+  float tn = orc_maxf(orc_maxf(orc_minf(ax, bx), orc_minf(ay, by)), orc_maxf(orc_minf(az, bz), t0));
+  float tf = orc_minf(orc_minf(orc_maxf(ax, bx), orc_maxf(ay, by)), orc_minf(orc_maxf(az, bz), t1));
+  return tn <= tf;
+}
+
+/* every particle whose (slightly inflated) sphere meets [t0, t1]: a superset of the particles
+ * that meet any bin inside the segment by the exact test of bin_contrib */
+static void seg_collect(const orc_scene *s, const orc_ray *ray, float t0, float t1, orc_cands *c) {
+  c->n = 0;
+  if (s->nleaves == 0) return;
+  float m = 1.0f;
+  for (int a = 0; a < 3; ++a) m = orc_maxf(m, orc_maxf(fabsf(ray->o[a]), fabsf(s->root_box[a])));
+  for (int a = 3; a < 6; ++a) m = orc_maxf(m, fabsf(s->root_box[a]));
+  const float e = m * 0x1p-14f;
+  float inv[3] = {1.0f / ray->d[0], 1.0f / ray->d[1], 1.0f / ray->d[2]};
+  uint32_t stack[128];
+  int sp = 0;
+  uint32_t todo[2];
+  int nt = 0;
+  if (s->root & ORC_LEAF_BIT) todo[nt++] = s->root;
+  else stack[sp++] = s->root;
+  for (;;) {
+    for (int k = 0; k < nt; ++k) {
+      uint32_t leaf = todo[k] & ~ORC_LEAF_BIT;
+      for (uint32_t j = 0; j < s->ppl; ++j) {
+        uint64_t i = (uint64_t)leaf * s->ppl + j;
+        if (i >= s->n) break;
+        const float *r = s->rec0 + 4 * i;
+        if (!(r[3] > 0.0f)) continue;
+        float vx = r[0] - ray->o[0], vy = r[1] - ray->o[1], vz = r[2] - ray->o[2];
+        float tc = (vx * ray->d[0] + vy * ray->d[1]) + vz * ray->d[2];
+        float wx = vx - tc * ray->d[0], wy = vy - tc * ray->d[1], wz = vz - tc * ray->d[2];
+        float h2 = (wx * wx + wy * wy) + wz * wz;
+        float R = r[3] * (1.0f + 0x1p-8f) + e;
+        if (h2 > R * R) continue;
+        float half = sqrtf(R * R - h2) + e;
+        if (tc + half < t0 || tc - half > t1) continue;
+        cands_push(c, (uint32_t)i);
+      }
+    }
+    nt = 0;
+    if (!sp) break;
+    uint32_t nd = stack[--sp];
+    uint32_t ch[2] = {s->left[nd], s->right[nd]};
+    for (int k = 0; k < 2; ++k) {
+      if (!seg_box_hit(child_box(s, ch[k]), ray, inv, t0, t1, e)) continue;
+      if (ch[k] & ORC_LEAF_BIT) todo[nt++] = ch[k];
+      else if (sp < 128) stack[sp++] = ch[k];
+      else abort();
+    }
+  }
+}
+
+/* a^3 rho at the closest approach of particle i to the ray segment [b0, b1], 0 when its sphere
+ * does not meet the segment */
+static float bin_contrib(const orc_scene *s, const orc_ray *ray, uint64_t i, float b0, float b1) {
+  const float *r = s->rec0 + 4 * i;
+  float vx = r[0] - ray->o[0], vy = r[1] - ray->o[1], vz = r[2] - ray->o[2];
+  float tc = (vx * ray->d[0] + vy * ray->d[1]) + vz * ray->d[2];
+  float wx = vx - tc * ray->d[0], wy = vy - tc * ray->d[1], wz = vz - tc * ray->d[2];
+  float h2 = (wx * wx + wy * wy) + wz * wz;
+  float tcl = orc_minf(orc_maxf(tc, b0), b1);
+  float dt = tcl - tc;
+  float d2 = h2 + dt * dt;
+  float r2 = r[3] * r[3];
+  if (!(d2 < r2)) return 0.0f;
+  float q2 = (9.0f * d2) / r2;
+  return orc_expf(-0.5f * q2) * s->w4[4 * i];
+}
+
+#define ORC_BIN_SPLIT_STEPS 4.0f /* split a bin while majorant * length exceeds this */
+#define ORC_BIN_SPLIT_DEPTH 10
+
+typedef struct {
+  const orc_scene *s;
+  const orc_params *p;
+  orc_tracker *tr;
+  const orc_ray *ray;
+  const orc_cands *c;
+  float scale, minf;
+} orc_bin_ctx;
+
+static float bin_majorant(const orc_bin_ctx *b, float lo, float hi) {
+  int64_t acc = 0;
+  for (size_t j = 0; j < b->c->n; ++j) acc += fix40(bin_contrib(b->s, b->ray, b->c->idx[j], lo, hi));
+  return ((float)acc * ORC_FIX_INV) * b->minf;
+}
+
+/* delta tracking across [lo, hi); a bin whose expected number of tentative steps exceeds
+ * ORC_BIN_SPLIT_STEPS is split in halves (front half first), at most ORC_BIN_SPLIT_DEPTH times.
+ * Returns 1 when the tracker is done (collision or step cap). */
+static int track_bin(const orc_bin_ctx *b, float lo, float hi, int depth, float *tp) {
+  float M = bin_majorant(b, lo, hi);
+  if (!(M > 0.0f)) return 0;
+  float mid = lo + 0.5f * (hi - lo);
+  if (M * (hi - lo) > ORC_BIN_SPLIT_STEPS && depth < ORC_BIN_SPLIT_DEPTH && mid > lo && mid < hi) {
+    if (track_bin(b, lo, mid, depth + 1, tp)) return 1;
+    return track_bin(b, mid, hi, depth + 1, tp);
+  }
+  orc_tracker *tr = b->tr;
+  const orc_ray *ray = b->ray;
+  float t = lo;
+  for (;;) {
+    if (tr->i >= ORC_MAX_DEPTH) {
+      *tp = t;
+      return 1;
+    }
+    tr->i += 1;
+    float u = orc_lcg_randomf(&tr->rng);
+    float step = -orc_logf(1.0f - u) / M;
+    t = t + step;
+    if (t >= hi || t >= ray->tmax) return 0;
+    float x[3] = {ray->o[0] + t * ray->d[0], ray->o[1] + t * ray->d[1], ray->o[2] + t * ray->d[2]};
+    orc_sample smp;
+    sample_at(b->s, x, &smp);
+    float sigma = smp.density * b->scale;
+    if (orc_lcg_randomf(&tr->rng) < sigma / M) {
+      float rgb[3];
+      sample_color(b->s, b->p, &smp, rgb);
+      tr->albedo[0] = rgb[0];
+      tr->albedo[1] = rgb[1];
+      tr->albedo[2] = rgb[2];
+      tr->albedo[3] = 1.0f;
+      *tp = t;
+      return 1;
+    }
+  }
+}
+
+static void track_majorant(const orc_scene *s, const orc_params *p, orc_tracker *tr, const orc_ray *ray) {
+  const float L = p->bin_length;
+  const float t0 = tr->t;
+  orc_cands c = {0, 0, 0};
+  orc_bin_ctx b = {s, p, tr, ray, &c, p->density_scale, p->density_scale * 1.0078125f};
+  /* (1 + 2^-7) on the majorant: slack for rounding in the bound */
+  int seg_end = 0; /* bins [.., seg_end) are covered by c */
+  int k = 0;
+  float t = t0;
+  for (;;) {
+    float b0 = t0 + (float)k * L;
+    float b1 = t0 + (float)(k + 1) * L;
+    if (!(b0 < ray->tmax) || !(b1 > b0)) break;
+    if (k >= seg_end) {
+      seg_collect(s, ray, b0, t0 + (float)(k + 16) * L, &c);
+      seg_end = k + 16;
+    }
+    float tp = b1;
+    if (track_bin(&b, b0, b1, 0, &tp)) {
+      tr->t = tp;
+      free(c.idx);
+      return;
+    }
+    k += 1;
+    t = b1;
+  }
+  tr->t = t;
+  free(c.idx);
+}
+
 static void track(const orc_scene *s, const orc_params *p, orc_tracker *tr, const orc_ray *ray,
                   int from_entry) {
   if (tr->marching) track_march(s, p, tr, ray);
+  else if (p->flags & ORC_FLAG_MAJORANT_TRACKING) track_majorant(s, p, tr, ray);
   else track_delta(s, p, tr, ray, from_entry);
 }
 

@@ -67,6 +67,7 @@ typedef struct orc_tf_desc {
   const float *color; int nc;    /* RGBA table, nc texels */
   const float *radius; int nr;   /* R table */
   const float *density; int nd;  /* R table */
+  float alpha_floor;             /* opacity below this counts as transparent (0: only alpha == 0) */
 } orc_tf_desc;
 
 /* xyzw: Hilbert-sorted particles with normalised attribute; radii may be NULL.
@@ -75,10 +76,11 @@ orc_scene *orc_scene_create(const float *xyzw, const float *radii, const uint64_
                             uint32_t ppl, float rbf_radius, const orc_tf_desc *tf);
 void orc_scene_destroy(orc_scene *s);
 uint32_t orc_scene_num_leaves(const orc_scene *s);
-/* copies out the BVH: left/right child codes (bit31 = leaf), internal boxes (6 floats each),
- * leaf boxes (6 floats each), root box (6 floats), per-particle eval record and weights */
+/* copies out the BVH: left/right child codes (bit31 = leaf), internal boxes (6 floats each;
+ * unions of the traversal leaf boxes), leaf boxes of the reference's bounds program, traversal
+ * leaf boxes (particles that can be hit), root box (6 floats) */
 void orc_scene_get_bvh(const orc_scene *s, uint32_t *left, uint32_t *right, float *node_box,
-                       float *leaf_box, float *root_box);
+                       float *leaf_box, float *leaf_eff, float *root_box);
 void orc_scene_get_prepass(const orc_scene *s, float *rec0, float *w4, float *rgeom);
 
 /* point query at x: returns hit count; acc = {D, R, G, B} fixed point (2^-40 units) */
@@ -92,7 +94,8 @@ enum {
   ORC_FLAG_VISUALIZE_ATTRIBUTES = 1u << 2,/* visualizeAttributes */
   ORC_FLAG_TRACK_FROM_ENTRY = 1u << 3,    /* native: tracking starts at tenter+unit*xi_y */
   ORC_FLAG_DENSITY_LINEAR = 1u << 4,      /* native: density = min(D*gain, 1) */
-  ORC_FLAG_SPLAT_PARTICLE_RADIUS = 1u << 5/* native: splat uses per-particle radius */
+  ORC_FLAG_SPLAT_PARTICLE_RADIUS = 1u << 5,/* native: splat uses per-particle radius */
+  ORC_FLAG_MAJORANT_TRACKING = 1u << 6    /* native: delta tracking with per-bin majorants */
 };
 
 typedef struct orc_params {
@@ -107,6 +110,8 @@ typedef struct orc_params {
   float aabb_min[3], aabb_max[3];
   float density_gain;
   float jitter_x, jitter_y;
+  float density_scale; /* majorant tracking: extinction = density_scale * D per unit length */
+  float bin_length;    /* majorant tracking: length of the majorant bins along a ray */
   const uint8_t *noise; /* RGBA8 atlas of 8x16 tiles of 256x256 (blue-noise mode) */
   int noise_w, noise_h;
 } orc_params;

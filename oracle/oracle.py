@@ -35,13 +35,15 @@ class OrcParams(ctypes.Structure):
         ("rbf_radius", ctypes.c_float), ("unit", ctypes.c_float),
         ("aabb_min", ctypes.c_float * 3), ("aabb_max", ctypes.c_float * 3),
         ("density_gain", ctypes.c_float), ("jitter_x", ctypes.c_float), ("jitter_y", ctypes.c_float),
+        ("density_scale", ctypes.c_float), ("bin_length", ctypes.c_float),
         ("noise", ctypes.c_void_p), ("noise_w", ctypes.c_int), ("noise_h", ctypes.c_int),
     ]
 
 
 class OrcTF(ctypes.Structure):
     _fields_ = [("color", ctypes.c_void_p), ("nc", ctypes.c_int), ("radius", ctypes.c_void_p),
-                ("nr", ctypes.c_int), ("density", ctypes.c_void_p), ("nd", ctypes.c_int)]
+                ("nr", ctypes.c_int), ("density", ctypes.c_void_p), ("nd", ctypes.c_int),
+                ("alpha_floor", ctypes.c_float)]
 
 
 def build():
@@ -78,7 +80,7 @@ def lib():
             "orc_scene_create": ([P, P, P, u64, u32, f32, ctypes.POINTER(OrcTF)], P),
             "orc_scene_destroy": ([P], None),
             "orc_scene_num_leaves": ([P], u32),
-            "orc_scene_get_bvh": ([P, P, P, P, P, P], None),
+            "orc_scene_get_bvh": ([P, P, P, P, P, P, P], None),
             "orc_scene_get_prepass": ([P, P, P, P], None),
             "orc_point_query": ([P, P, P], i32),
             "orc_point_query_brute": ([P, P, P], i32),
@@ -155,7 +157,7 @@ def tf_from_rgba8(cm, rm, dm):
 class Scene:
     """Prepass + leaf bounds + LBVH of Hilbert-sorted particles (as aarbf_build leaves them)."""
 
-    def __init__(self, sorted_xyzw, sorted_radii, keys, ppl, rbf_radius, tf):
+    def __init__(self, sorted_xyzw, sorted_radii, keys, ppl, rbf_radius, tf, alpha_floor=0.0):
         self.xyzw = np.ascontiguousarray(sorted_xyzw, np.float32)
         self.radii = None if sorted_radii is None else np.ascontiguousarray(sorted_radii, np.float32)
         self.keys = np.ascontiguousarray(keys, np.uint64)
@@ -164,7 +166,7 @@ class Scene:
                            np.ascontiguousarray(rm, np.float32).reshape(-1),
                            np.ascontiguousarray(dm, np.float32).reshape(-1))
         c, r, d = self._tf_arrays
-        t = OrcTF(c.ctypes.data, len(c), r.ctypes.data, len(r), d.ctypes.data, len(d))
+        t = OrcTF(c.ctypes.data, len(c), r.ctypes.data, len(r), d.ctypes.data, len(d), float(alpha_floor))
         self.n = len(self.xyzw)
         self.h = lib().orc_scene_create(_p(self.xyzw), _p(self.radii), _p(self.keys), self.n, int(ppl),
                                         float(rbf_radius), ctypes.byref(t))
@@ -181,9 +183,10 @@ class Scene:
         right = np.zeros(ni, np.uint32)
         nb = np.zeros((ni, 6), np.float32)
         lb = np.zeros((self.nleaves, 6), np.float32)
+        le = np.zeros((self.nleaves, 6), np.float32)
         rb = np.zeros(6, np.float32)
-        lib().orc_scene_get_bvh(self.h, _p(left), _p(right), _p(nb), _p(lb), _p(rb))
-        return left, right, nb, lb, rb
+        lib().orc_scene_get_bvh(self.h, _p(left), _p(right), _p(nb), _p(lb), _p(le), _p(rb))
+        return left, right, nb, lb, le, rb
 
     def prepass(self):
         rec0 = np.zeros((self.n, 4), np.float32)
@@ -219,13 +222,13 @@ class Scene:
         return image
 
 
-def build_scene(xyzw, radii, dom, ppl, rbf_radius, tf):
+def build_scene(xyzw, radii, dom, ppl, rbf_radius, tf, alpha_floor=0.0):
     """The whole build pipeline on the CPU: keys, sort, gather/normalise, scene."""
     xyzw = np.ascontiguousarray(xyzw, np.float32)
     keys = hilbert_keys(xyzw, dom)
     perm = sort_perm(keys, xyzw)
     sx, sr = gather_normalize(xyzw, radii, perm, dom[6], dom[7])
-    return Scene(sx, sr, keys[perm], ppl, rbf_radius, tf), keys[perm], perm
+    return Scene(sx, sr, keys[perm], ppl, rbf_radius, tf, alpha_floor), keys[perm], perm
 
 
 def taa(image, prev, disable=False):
@@ -254,6 +257,8 @@ def params_from(rp, noise=None):
         getattr(p, name)[:] = [float(np.float32(v)) for v in getattr(rp, name)]
     p.rbf_radius, p.unit, p.density_gain = rp.rbf_radius, rp.unit, rp.density_gain
     p.jitter_x, p.jitter_y = rp.jitter_x, rp.jitter_y
+    p.density_scale = getattr(rp, "density_scale", 0.0)
+    p.bin_length = getattr(rp, "bin_length", 0.0)
     if noise is not None:
         p.noise = noise.ctypes.data
         p.noise_h, p.noise_w = noise.shape[0], noise.shape[1]

@@ -12,6 +12,8 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
+BVH_PARTS = ("left", "right", "node boxes", "bounds-program leaf boxes", "traversal leaf boxes", "root box")
+
 
 def bits(a):
     a = np.ascontiguousarray(a)
@@ -81,10 +83,11 @@ def random_scene(n, seed, dup=0, radii=False):
     return xyzw, r
 
 
-def setup_both(ctx, orc, aarbf_mod, xyzw, radii, ppl, rbf, tf8=None, tf32=None):
+def setup_both(ctx, orc, aarbf_mod, xyzw, radii, ppl, rbf, tf8=None, tf32=None, alpha_floor=0.0):
     dom = orc.domain([xyzw])
     ctx.set_particles(xyzw, radii)
     ctx.set_domain(dom)
+    ctx.set_opacity_floor(alpha_floor)
     if tf32 is not None:
         ctx.set_transfer_functions_f32(*tf32)
         tf = tf32
@@ -93,7 +96,7 @@ def setup_both(ctx, orc, aarbf_mod, xyzw, radii, ppl, rbf, tf8=None, tf32=None):
         ctx.set_transfer_functions_rgba8(*tf8)
         tf = orc.tf_from_rgba8(*tf8)
     ctx.build(rbf, ppl)
-    scene, keys, perm = orc.build_scene(xyzw, radii, dom, ppl, rbf, tf)
+    scene, keys, perm = orc.build_scene(xyzw, radii, dom, ppl, rbf, tf, alpha_floor)
     return scene, keys, perm, dom
 
 
@@ -108,7 +111,7 @@ def test_build_bitexact(ctx, orc, aarbf_mod, n, ppl, dup):
     assert_bitexact(ctx.sorted_particles(), scene.xyzw, "sorted particles")
     for g, w, name in zip(ctx.prepass(), scene.prepass(), ("rec0", "w4", "rgeom")):
         assert_bitexact(g, w, name)
-    for g, w, name in zip(ctx.bvh(), scene.bvh(), ("left", "right", "node boxes", "leaf boxes", "root box")):
+    for g, w, name in zip(ctx.bvh(), scene.bvh(), BVH_PARTS):
         assert_bitexact(g, w, name)
 
 
@@ -211,16 +214,38 @@ def test_render_marching_blue_noise(ctx, orc, aarbf_mod, traversal):
 def test_render_native_mode(ctx, orc, aarbf_mod, traversal):
     from aarbf import scenes
     sc = scenes.config_clusters(30_000, clusters=8, seed=5)
-    cm, rm, dm = scenes.tf_four_peaks()
+    cm, rm, dm = scenes.tf_linear_ramp()
     dom = orc.domain([sc.xyzw])
     w, h = 40, 30
     cam = scenes.orbit_camera()
-    rp = scenes.native_params(cam, w, h, float(sc.radii.max()), 0.002, 50.0, dom, spp=2, traversal=traversal)
+    rp = scenes.native_params(cam, w, h, float(sc.radii.max()), 0.002, 2000.0, dom, spp=2, traversal=traversal)
     scene, *_ = setup_both(ctx, orc, aarbf_mod, sc.xyzw, sc.radii, 1, rp.rbf_radius, tf32=(cm, rm, dm))
     ga, gi = gpu_render(ctx, rp, w, h)
     oa, oi = scene.render(orc.params_from(rp), w, h)
     assert_radiance(gi, oi, "image")
-    assert (oi[..., :3] > 0).mean() > 0.05
+    assert (oi[..., :3] > 0).mean() > 0.01  # the view is not empty
+
+
+@pytest.mark.parametrize("n,ppl,bins,scale,floor", [(30_000, 1, 4.0, 200.0, 0.0), (30_000, 4, 1.0, 200.0, 0.0),
+                                                    (200_000, 1, 8.0, 200.0, 1 / 255),
+                                                    (200_000, 8, 32.0, 5000.0, 1 / 255)])
+def test_render_majorant_tracking(ctx, orc, aarbf_mod, n, ppl, bins, scale, floor):
+    """delta tracking with per-bin majorants (native extinction density_scale * D); the dense
+    case exercises the bin refinement and the direct (unstaged) bins"""
+    from aarbf import scenes
+    sc = scenes.config_clusters(n, clusters=8, seed=6)
+    cm, rm, dm = scenes.tf_linear_ramp()
+    dom = orc.domain([sc.xyzw])
+    w, h = 40, 30
+    rp = scenes.native_params(scenes.orbit_camera(), w, h, float(sc.radii.max()), 0.002, scale, dom, spp=2,
+                              majorant=True, bin_length=bins * 0.002)
+    scene, *_ = setup_both(ctx, orc, aarbf_mod, sc.xyzw, sc.radii, ppl, rp.rbf_radius, tf32=(cm, rm, dm),
+                           alpha_floor=floor)
+    ga, gi = gpu_render(ctx, rp, w, h)
+    oa, oi = scene.render(orc.params_from(rp), w, h)
+    assert_radiance(gi, oi, "image")
+    assert_radiance(ga, oa, "accum")
+    assert (oi[..., :3] > 0).mean() > 0.01  # the view is not empty
 
 
 @pytest.mark.parametrize("native", [False, True])
@@ -242,7 +267,7 @@ def test_splat_parity(ctx, orc, aarbf_mod, native):
     _, gi = gpu_render(ctx, rp, w, h, splat=True)
     oi = scene.render_splat(orc.params_from(rp), w, h)
     assert_radiance(gi, oi, "splat image")
-    assert (oi[..., :3] > 0).mean() > 0.05
+    assert (oi[..., :3] > 0).mean() > 0.01  # the view is not empty
 
 
 def test_taa_parity(ctx, orc):
@@ -318,7 +343,7 @@ def test_edge_cases(ctx, orc, aarbf_mod, case):
         return
     ctx.set_domain(dom)
     scene, keys, perm, _ = setup_both(ctx, orc, aarbf_mod, xyzw, None, ppl, r, tf8=tf8)
-    for g, wv, name in zip(ctx.bvh(), scene.bvh(), ("left", "right", "node boxes", "leaf boxes", "root")):
+    for g, wv, name in zip(ctx.bvh(), scene.bvh(), BVH_PARTS):
         assert_bitexact(g, wv, name)
     for trav in (0, 1):
         rp.traversal = trav
@@ -341,7 +366,7 @@ def test_refit_after_transfer_function_change(ctx, orc, aarbf_mod):
         ctx.render(rp, w, h)          # prepass is stale until refit
     ctx.refit(r * 1.5)
     scene, *_ = orc.build_scene(xyzw, None, dom, 2, r * 1.5, orc.tf_from_rgba8(cm, rm, dm))
-    for g, wv, name in zip(ctx.bvh(), scene.bvh(), ("left", "right", "node boxes", "leaf boxes", "root")):
+    for g, wv, name in zip(ctx.bvh(), scene.bvh(), BVH_PARTS):
         assert_bitexact(g, wv, name)
     rp.rbf_radius = r * 1.5
     ga, gi = gpu_render(ctx, rp, w, h)
@@ -363,7 +388,7 @@ def test_full_size_properties(ctx, orc, aarbf_mod):
     k, p = ctx.hilbert_keys()
     assert (np.diff(k.astype(np.int64)) >= 0).all()
     assert np.array_equal(np.sort(p), np.arange(len(p), dtype=np.uint32))
-    left, right, nb, lb, rb = ctx.bvh()
+    left, right, nb, _, lb, rb = ctx.bvh()
     # every child box lies inside its parent's box
     LEAF = np.uint32(0x80000000)
     for ch in (left, right):
@@ -379,7 +404,7 @@ def test_full_size_properties(ctx, orc, aarbf_mod):
         rp.traversal = trav
         imgs.append(gpu_render(ctx, rp, w, h)[1])
     assert_bitexact(imgs[0], imgs[1], "staged vs point at 10M")
-    assert (imgs[0][..., :3] > 0).mean() > 0.05
+    assert (imgs[0][..., :3] > 0).mean() > 0.01
 
 
 def test_oracle_parity_1m(ctx, orc, aarbf_mod):
@@ -390,7 +415,13 @@ def test_oracle_parity_1m(ctx, orc, aarbf_mod):
     w, h = 48, 32
     dom = orc.domain([sc.xyzw])
     rp = scenes.native_params(scenes.orbit_camera(), w, h, float(sc.radii.max()), 0.001, 50.0, dom, spp=1)
-    scene, *_ = setup_both(ctx, orc, aarbf_mod, sc.xyzw, sc.radii, 1, rp.rbf_radius, tf32=(cm, rm, dm))
+    scene, *_ = setup_both(ctx, orc, aarbf_mod, sc.xyzw, sc.radii, 8, rp.rbf_radius, tf32=(cm, rm, dm),
+                           alpha_floor=1 / 255)
     ga, gi = gpu_render(ctx, rp, w, h)
     oa, oi = scene.render(orc.params_from(rp), w, h)
     assert_radiance(gi, oi, "1M image")
+    rpm = scenes.native_params(scenes.orbit_camera(), w, h, float(sc.radii.max()), 0.001, 50.0, dom, spp=2,
+                               majorant=True, bin_length=0.016)
+    ga, gi = gpu_render(ctx, rpm, w, h)
+    oa, oi = scene.render(orc.params_from(rpm), w, h)
+    assert_radiance(gi, oi, "1M image, majorant tracking")
