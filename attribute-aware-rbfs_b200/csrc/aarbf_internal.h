@@ -74,6 +74,8 @@ struct RenderLaunch {
   float density_scale, bin_length; // majorant tracking
   uint32_t* work_counter;          // persistent kernel: next pixel tile item (zeroed per launch)
   int candidate_cap;               // staging buffer depth per ray (template instance)
+  float4* samples;                 // spp planes of per-sample colours (width * height each)
+  float* noise_buf;                // per pixel: noise value of the last sample (showNoise)
 };
 
 // launchers (defined in the .cu files)
@@ -140,7 +142,7 @@ struct aarbf_ctx {
   // framebuffers owned by the context
   aarbf::DevBuf fb_accum, fb_image;
   int fb_w = 0, fb_h = 0;
-  // status word, persistent-kernel work counter
-  aarbf::DevBuf status, work;
+  // status word, persistent-kernel work counter, per-sample colour planes
+  aarbf::DevBuf status, work, samples, noise_buf;
   float max_radius = 0.0f;
 };

@@ -222,6 +222,10 @@ aarbf_status fill_launch(aarbf_ctx* ctx, const aarbf_params* p, int w, int h, fl
     return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "majorant tracking needs bin_length > 0, density_scale >= 0");
   if (!ctx->work.ptr) CK(ctx->work.reserve(256), "work counter");
   L.work_counter = ctx->work.as<uint32_t>();
+  CK(ctx->samples.reserve(sizeof(float) * 4 * (size_t)w * (size_t)h * L.spp), "sample planes");
+  CK(ctx->noise_buf.reserve(sizeof(float) * (size_t)w * (size_t)h), "noise plane");
+  L.samples = ctx->samples.as<float4>();
+  L.noise_buf = ctx->noise_buf.as<float>();
   return AARBF_OK;
 }
 
@@ -290,7 +294,8 @@ aarbf_status aarbf_destroy(aarbf_ctx* ctx) {
                     &ctx->rgeom, &ctx->nodes, &ctx->nodes_ref, &ctx->leaf_eff, &ctx->leaf_parent, &ctx->counters,
                     &ctx->leaf_box, &ctx->root_box,
                     &ctx->sorted_keys, &ctx->tf_color, &ctx->tf_radius, &ctx->tf_density, &ctx->noise,
-                    &ctx->fb_accum, &ctx->fb_image, &ctx->status, &ctx->work};
+                    &ctx->fb_accum, &ctx->fb_image, &ctx->status, &ctx->work, &ctx->samples,
+                    &ctx->noise_buf};
   for (DevBuf* b : bufs) b->release();
   delete ctx;
   return AARBF_OK;

@@ -758,47 +758,70 @@ __device__ float4 raygen_sample(const RenderLaunch& L, uint32_t frame, int px, i
   return over4(color, make_float4(0.0f, 0.0f, 0.0f, 1.0f));
 }
 
-// Persistent kernel: each thread repeatedly takes the next pixel from a global counter (32
-// consecutive items form an 8x4 pixel tile) and renders all of its samples, so long rays no
-// longer hold up the rest of a statically assigned tile.
+// Persistent kernel: each thread repeatedly takes the next work item from a global counter.
+// An item is one sample of one pixel; 32 consecutive items are one sample of an 8x4 pixel tile
+// and the spp groups of a tile follow each other, so the samples of an expensive pixel run on
+// different threads at the same time. Each sample's colour goes to its own plane of L.samples;
+// k_accumulate then forms the running mean in sample order (bit-identical to spp launches).
 template <int CAP>
 __global__ void __launch_bounds__(kBlock) k_render(const RenderLaunch L) {
   extern __shared__ __align__(16) char smem[];
   const uint32_t tiles_x = (uint32_t)(L.width + 7) / 8u;
-  const uint32_t total = tiles_x * ((uint32_t)(L.height + 3) / 4u) * 32u;
   const uint32_t spp = L.spp ? L.spp : 1u;
+  const uint32_t total = tiles_x * ((uint32_t)(L.height + 3) / 4u) * 32u * spp;
+  const size_t plane = (size_t)L.width * (size_t)L.height;
+  const bool cost = (L.flags & kFlagCostImage) != 0;
   for (;;) {
     uint32_t item = atomicAdd(L.work_counter, 1u);
     if (item >= total) break;
-    uint32_t tile = item >> 5, in = item & 31u;
+    uint32_t group = item >> 5, in = item & 31u;
+    uint32_t tile = group / spp, k = group % spp;
     const int px = (int)((tile % tiles_x) * 8u + (in & 7u));
     const int py = (int)((tile / tiles_x) * 4u + (in >> 3));
     if (px >= L.width || py >= L.height) continue;
     const size_t ofs = (size_t)px + (size_t)L.width * (size_t)py;
-    float4 prev = L.accum[ofs];
-    float4 fin = prev;
-    float noise = 0.0f;
-    const bool cost = (L.flags & kFlagCostImage) != 0;
     const long long c0 = cost ? clock64() : 0;
-    for (uint32_t k = 0; k < spp; ++k) {
-      uint32_t frame = (L.frame_id + k) & 0xffffu;
-      uint32_t aid = (L.accum_id + k) & 0xffffu;
-      float4 c = raygen_sample<CAP>(L, frame, px, py, noise, smem);
-      // running mean, deviceCodeRBF.hlsl:326-328
-      float fa = (float)aid;
-      float wa = 1.0f / fa, wb = (float)((int)aid - 1) / fa;
-      fin.x = wa * c.x + wb * prev.x;
-      fin.y = wa * c.y + wb * prev.y;
-      fin.z = wa * c.z + wb * prev.z;
-      fin.w = wa * c.w + wb * prev.w;
-      prev = fin;
-    }
-    L.accum[ofs] = fin;
-    if (L.flags & kFlagShowNoise) fin = make_float4(noise, noise, noise, 1.0f);
-    // diagnostic: the image's alpha channel receives the pixel's cost in SM clock cycles
-    if (cost) fin.w = (float)(clock64() - c0);
-    L.image[ofs] = fin;
+    float noise = 0.0f;
+    float4 c = raygen_sample<CAP>(L, (L.frame_id + k) & 0xffffu, px, py, noise, smem);
+    if (cost) c.w = (float)(clock64() - c0);
+    L.samples[(size_t)k * plane + ofs] = c;
+    if (k + 1 == spp) L.noise_buf[ofs] = noise;
   }
+}
+
+// running mean over the samples in order, deviceCodeRBF.hlsl:326-335
+__global__ void k_accumulate(const RenderLaunch L) {
+  const size_t plane = (size_t)L.width * (size_t)L.height;
+  const size_t ofs = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (ofs >= plane) return;
+  const uint32_t spp = L.spp ? L.spp : 1u;
+  const bool cost = (L.flags & kFlagCostImage) != 0;
+  float4 prev = L.accum[ofs];
+  float4 fin = prev;
+  float cycles = 0.0f;
+  for (uint32_t k = 0; k < spp; ++k) {
+    float4 c = L.samples[(size_t)k * plane + ofs];
+    if (cost) {
+      cycles += c.w;
+      c.w = 1.0f;
+    }
+    uint32_t aid = (L.accum_id + k) & 0xffffu;
+    float fa = (float)aid;
+    float wa = 1.0f / fa, wb = (float)((int)aid - 1) / fa;
+    fin.x = wa * c.x + wb * prev.x;
+    fin.y = wa * c.y + wb * prev.y;
+    fin.z = wa * c.z + wb * prev.z;
+    fin.w = wa * c.w + wb * prev.w;
+    prev = fin;
+  }
+  L.accum[ofs] = fin;
+  if (L.flags & kFlagShowNoise) {
+    float noise = L.noise_buf[ofs];
+    fin = make_float4(noise, noise, noise, 1.0f);
+  }
+  // diagnostic: the image's alpha channel receives the pixel's cost in SM clock cycles
+  if (cost) fin.w = cycles;
+  L.image[ofs] = fin;
 }
 
 template <int CAP>
@@ -817,10 +840,14 @@ cudaError_t launch_cap(const RenderLaunch& L, cudaStream_t st) {
   }
   cudaError_t e = cudaMemsetAsync(L.work_counter, 0, sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
-  uint32_t tiles = (uint32_t)((L.width + 7) / 8) * (uint32_t)((L.height + 3) / 4);
-  int grid = (int)(tiles * 32u + kBlock - 1) / kBlock;
+  uint64_t items = (uint64_t)((L.width + 7) / 8) * (uint64_t)((L.height + 3) / 4) * 32u * (L.spp ? L.spp : 1u);
+  int grid = (int)((items + kBlock - 1) / kBlock);
   if (grid > blocks) grid = blocks;
   k_render<CAP><<<grid, kBlock, smem, st>>>(L);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  size_t plane = (size_t)L.width * (size_t)L.height;
+  k_accumulate<<<(unsigned)((plane + 255) / 256), 256, 0, st>>>(L);
   return cudaGetLastError();
 }
 
