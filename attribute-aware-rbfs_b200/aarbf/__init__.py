@@ -52,6 +52,7 @@ EXPORTED_SYMBOLS = (
     "aarbf_get_num_particles", "aarbf_get_hilbert_keys", "aarbf_get_sorted_particles",
     "aarbf_get_prepass", "aarbf_get_bvh", "aarbf_device_alloc", "aarbf_device_free",
     "aarbf_memcpy", "aarbf_memset", "aarbf_render_count", "aarbf_set_opacity_floor",
+    "aarbf_hilbert_sort_noalloc",
 )
 
 
@@ -116,6 +117,7 @@ def _load():
         "aarbf_get_prepass": [P, P, P, P],
         "aarbf_get_bvh": [P, P, P, P, P, P, P],
         "aarbf_set_opacity_floor": [P, f32],
+        "aarbf_hilbert_sort_noalloc": [P, u64, P, P, P, P],
         "aarbf_get_version": [ctypes.POINTER(i32), ctypes.POINTER(i32)],
         "aarbf_device_alloc": [P, ctypes.c_size_t, ctypes.POINTER(P)],
         "aarbf_device_free": [P, P],
@@ -209,6 +211,20 @@ def generate_noise_atlas(width: int = 2048, height: int = 4096) -> np.ndarray:
     if st:
         raise AarbfError(st)
     return out
+
+
+#: largest particle count aarbf_hilbert_sort_noalloc accepts (include/aarbf.h)
+NOALLOC_MAX_PARTICLES = 1 << 20
+
+
+def hilbert_sort_noalloc(xyzw_dev: int, n: int, dom, keys_dev: int, perm_dev: int, stream=None):
+    """aarbf_hilbert_sort_noalloc: Hilbert keys and sort permutation of n device-resident
+    particles into caller-provided device outputs, without allocating device memory."""
+    d = np.ascontiguousarray(dom, np.float32)
+    st = lib().aarbf_hilbert_sort_noalloc(_ptr(xyzw_dev), int(n), _ptr(d), _ptr(keys_dev), _ptr(perm_dev),
+                                          _stream_ptr(stream))
+    if st:
+        raise AarbfError(st, "aarbf_hilbert_sort_noalloc")
 
 
 def domain_init() -> np.ndarray:

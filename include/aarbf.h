@@ -210,6 +210,24 @@ aarbf_status aarbf_series_free(aarbf_series *s);
 aarbf_status aarbf_series_save(const char *path, const float *const *frames, const uint64_t *counts,
                                uint64_t nframes);
 
+/* ---- allocation-free Hilbert sort ---------------------------------------------------------- */
+
+/* No counterpart in the reference. For callers that cannot allocate device memory -- code run
+ * while a CUDA graph is being captured, memory managed by a pool or arena that forbids other
+ * allocations, real-time loops that must not touch the allocator: the Hilbert keys and sort
+ * permutation that aarbf_build computes, without calling cudaMalloc or cudaFree. xyzw: device
+ * pointer to n float4 particles; dom: HOST pointer to the 8-float domain of aarbf_set_domain;
+ * keys (n x u64) and perm (n x u32): device outputs, equal to aarbf_get_hilbert_keys' results.
+ * Working space is a fixed array in device memory that every GPU loading the library holds
+ * until the process exits (about 12.5 MiB), so n is limited to AARBF_NOALLOC_MAX_PARTICLES;
+ * larger n returns AARBF_ERR_INVALID_ARGUMENT. All calls share that array: calls whose GPU work
+ * overlaps (other streams, other host threads) race and must be ordered by the caller. The first
+ * call on a device looks up the array's address; make it before any stream capture. The call
+ * synchronises `stream` once (to read the tie flag), like aarbf_build. */
+#define AARBF_NOALLOC_MAX_PARTICLES (1u << 20)
+aarbf_status aarbf_hilbert_sort_noalloc(const float *xyzw, uint64_t n, const float *dom,
+                                        uint64_t *keys, uint32_t *perm, void *stream);
+
 /* ---- debug getters (bit-exact tests) ------------------------------------------------------ */
 
 aarbf_status aarbf_get_num_particles(const aarbf_ctx *ctx, uint64_t *n, uint32_t *num_leaves);
