@@ -258,6 +258,7 @@ def main():
     import torch.distributed as dist
 
     import aarbf
+    from aarbf import replicas
 
     rank, local_rank, world = dist_env()
     if world > 1:
@@ -284,7 +285,7 @@ def main():
     image = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)
 
     def step(k):
-        rp = params_for(args, dom, rmax, frame_id=(k * S + rank * 7919) & 0xFFFF)
+        rp = params_for(args, dom, rmax, frame_id=replicas.frame_id(rank, k, S))
         ctx.render(rp, W, H, accum, image, stream=sp)
 
     for k in range(args.warmup):

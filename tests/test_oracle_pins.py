@@ -158,6 +158,24 @@ def test_taa_constant_image_is_fixed_point(orc):
     assert (bgra == ((255 << 24) | (int(0.3 * 255 + .5) << 16) | (int(0.6 * 255 + .5) << 8) | int(0.2 * 255 + .5))).all()
 
 
+def test_majorant_estimator_is_unbiased(orc):
+    """delta tracking with per-bin majorants converges to the plain estimator's image where the
+    plain estimator's global majorant (1 per unit) bounds the extinction (no clamping)"""
+    from aarbf import scenes
+    sc = scenes.config_clusters(20_000, clusters=8, seed=6)
+    tf = scenes.tf_linear_ramp()
+    dom = orc.domain([sc.xyzw])
+    scene, _, _ = orc.build_scene(sc.xyzw, sc.radii, dom, 1, float(sc.radii.max()), tf)
+    means = []
+    for majorant in (False, True):
+        rp = scenes.native_params(scenes.orbit_camera(), 32, 24, float(sc.radii.max()), 0.001, 20.0, dom,
+                                  spp=192, majorant=majorant, bin_length=0.008)
+        _, img = scene.render(orc.params_from(rp), 32, 24)
+        means.append(img[..., :3].astype(np.float64).mean())
+    assert means[0] > 0
+    assert abs(means[1] - means[0]) < 0.03 * means[0]
+
+
 def test_sort_tie_break(orc):
     """equal Hilbert keys are ordered by (x, y, z, w) then input index"""
     xyzw = np.array([[0.5, 0.5, 0.5, 0.9], [0.5, 0.5, 0.5, 0.1], [0.0, 0.0, 0.0, 0.0], [1, 1, 1, 1],
