@@ -32,8 +32,10 @@ FLAG_DENSITY_LINEAR = 1 << 4
 FLAG_SPLAT_PARTICLE_RADIUS = 1 << 5
 FLAG_MAJORANT_TRACKING = 1 << 6
 
+TRAVERSAL_AUTO = 0      # majorant tracking: one warp per ray; otherwise per-thread staged
 TRAVERSAL_STAGED = 0
-TRAVERSAL_POINT = 1
+TRAVERSAL_POINT = 1     # one BVH point query per tracking step
+TRAVERSAL_THREAD = 2    # per-thread staged segments for every estimator
 
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "out of memory", 3: "CUDA error",

@@ -76,6 +76,7 @@ struct RenderLaunch {
   int candidate_cap;               // staging buffer depth per ray (template instance)
   float4* samples;                 // spp planes of per-sample colours (width * height each)
   float* noise_buf;                // per pixel: noise value of the last sample (showNoise)
+  uint32_t* warp_stacks;           // ray-per-warp kernel: one traversal stack per resident warp
 };
 
 // launchers (defined in the .cu files)
@@ -105,6 +106,8 @@ cudaError_t launch_refit(const float4* rec0, const float* rgeom, uint64_t n, uin
                          uint32_t* counters, float* leaf_box, float* leaf_eff, float* root_box,
                          cudaStream_t st);
 cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st);
+bool render_uses_warp_kernel(const RenderLaunch& L);
+cudaError_t render_warp_stack_words(size_t* words);
 cudaError_t launch_splat(const RenderLaunch& L, cudaStream_t st);
 cudaError_t launch_taa(const float4* image, const float4* prev, float4* taa, uint32_t* bgra, int w,
                        int h, int disable, cudaStream_t st);
@@ -143,6 +146,6 @@ struct aarbf_ctx {
   aarbf::DevBuf fb_accum, fb_image;
   int fb_w = 0, fb_h = 0;
   // status word, persistent-kernel work counter, per-sample colour planes
-  aarbf::DevBuf status, work, samples, noise_buf;
+  aarbf::DevBuf status, work, samples, noise_buf, warp_stacks;
   float max_radius = 0.0f;
 };

@@ -226,6 +226,12 @@ aarbf_status fill_launch(aarbf_ctx* ctx, const aarbf_params* p, int w, int h, fl
   CK(ctx->noise_buf.reserve(sizeof(float) * (size_t)w * (size_t)h), "noise plane");
   L.samples = ctx->samples.as<float4>();
   L.noise_buf = ctx->noise_buf.as<float>();
+  if (render_uses_warp_kernel(L)) {
+    size_t words = 0;
+    CK(render_warp_stack_words(&words), "warp kernel setup");
+    CK(ctx->warp_stacks.reserve(4 * words), "warp stacks");
+    L.warp_stacks = ctx->warp_stacks.as<uint32_t>();
+  }
   return AARBF_OK;
 }
 
@@ -295,7 +301,7 @@ aarbf_status aarbf_destroy(aarbf_ctx* ctx) {
                     &ctx->leaf_box, &ctx->root_box,
                     &ctx->sorted_keys, &ctx->tf_color, &ctx->tf_radius, &ctx->tf_density, &ctx->noise,
                     &ctx->fb_accum, &ctx->fb_image, &ctx->status, &ctx->work, &ctx->samples,
-                    &ctx->noise_buf};
+                    &ctx->noise_buf, &ctx->warp_stacks};
   for (DevBuf* b : bufs) b->release();
   delete ctx;
   return AARBF_OK;

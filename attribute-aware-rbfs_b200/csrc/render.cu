@@ -674,9 +674,11 @@ __device__ __forceinline__ void track(const RenderLaunch& L, Tracker& tr, const 
   ctr_add(L.counters, kCtrSteps, (unsigned long long)(tr.i - i0 + 1));
 }
 
-// ParticleRBFRayGen body for one sample (deviceCodeRBF.hlsl:206-324)
-template <int CAP>
-__device__ float4 raygen_sample(const RenderLaunch& L, uint32_t frame, int px, int py, float& noise, char* smem) {
+// ParticleRBFRayGen body for one sample (deviceCodeRBF.hlsl:206-324); track_fn runs the tracker
+// (per thread or per warp), count_lane selects the lane that does count-mode accounting
+template <class TrackFn>
+__device__ float4 raygen_generic(const RenderLaunch& L, uint32_t frame, int px, int py, float& noise,
+                                 bool count_lane, TrackFn&& track_fn) {
   uint32_t rng = pixel_seed(frame, (uint32_t)px, (uint32_t)py, (uint32_t)L.width);
   float sx = ((float)px + 0.5f + L.jitter_x) / (float)L.width;
   float sy = ((float)py + 0.5f + L.jitter_y) / (float)L.height;
@@ -725,10 +727,10 @@ __device__ float4 raygen_sample(const RenderLaunch& L, uint32_t frame, int px, i
     tr.t = tenter + L.unit * r1;
     const bool from_entry = (L.flags & kFlagTrackFromEntry) != 0;
     const float t_start = (blue || from_entry) ? tr.t : ray.tmin;
-    track<CAP>(L, tr, ray, from_entry, smem);
+    track_fn(tr, ray, from_entry);
     float4 albedo = tr.albedo;
     float t = tr.t;
-    if (L.counters) count_segment(L, ray, t_start, fminf(t, ray.tmax));
+    if (L.counters && count_lane) count_segment(L, ray, t_start, fminf(t, ray.tmax));
     float vis = 1.0f;
     if (albedo.w > 0.0f && L.ambient != 1.0f) {
       Ray sr;
@@ -744,9 +746,9 @@ __device__ float4 raygen_sample(const RenderLaunch& L, uint32_t frame, int px, i
       tr.shadow = true;
       tr.t = blue ? -L.unit * r2 : 0.0f;
       const float ts0 = tr.t;
-      track<CAP>(L, tr, sr, false, smem);
+      track_fn(tr, sr, false);
       vis = 1.0f - tr.albedo.w;
-      if (L.counters) count_segment(L, sr, fmaxf(ts0, 0.0f), fminf(tr.t, sr.tmax));
+      if (L.counters && count_lane) count_segment(L, sr, fmaxf(ts0, 0.0f), fminf(tr.t, sr.tmax));
     }
     if (albedo.w == 1.0f) {
       color.x = (albedo.x * vis) * (1.0f - L.ambient) + albedo.x * L.ambient;
@@ -756,6 +758,405 @@ __device__ float4 raygen_sample(const RenderLaunch& L, uint32_t frame, int px, i
     }
   }
   return over4(color, make_float4(0.0f, 0.0f, 0.0f, 1.0f));
+}
+
+template <int CAP>
+__device__ float4 raygen_sample(const RenderLaunch& L, uint32_t frame, int px, int py, float& noise, char* smem) {
+  return raygen_generic(L, frame, px, py, noise, true,
+                        [&](Tracker& tr, const Ray& r, bool from_entry) { track<CAP>(L, tr, r, from_entry, smem); });
+}
+
+// ============================================================================================
+// Ray-per-warp kernel for majorant tracking. All 32 lanes of a warp work on one ray: the
+// sequential tracker logic runs uniformly on every lane (identical values), and the heavy parts
+// are split across lanes -- BVH traversal as a warp-wide frontier compacted with ballots,
+// candidate staging into a per-warp shared buffer, and the fixed-point sums of majorants and
+// densities, which lanes accumulate over disjoint particles and combine with shuffles (integer
+// sums, so the lane split cannot change a bit).
+// ============================================================================================
+
+constexpr int kWarpCap = 1024;        // staged candidates per ray (per warp)
+constexpr int kWarpsPerBlock = 4;
+constexpr int kWarpStack = 8192;      // traversal stack entries per warp (global memory)
+constexpr unsigned kFull = 0xffffffffu;
+
+struct WarpBuf {
+  uint32_t idx[kWarpCap];
+  float lo[kWarpCap];
+  float hi[kWarpCap];
+  uint32_t leaves[64];
+};
+
+__device__ __forceinline__ uint32_t lane_lt_mask() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ long long warp_sum(long long v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+__device__ __forceinline__ int warp_sum(int v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v = fminf(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+
+__device__ __forceinline__ void warp_sum_sample(Sample& s) {
+  s.count = warp_sum(s.count);
+  s.a0 = warp_sum(s.a0);
+  s.a1 = warp_sum(s.a1);
+  s.a2 = warp_sum(s.a2);
+  s.a3 = warp_sum(s.a3);
+}
+
+// Warp-wide traversal of the (traversal-bounds) BVH. box_test(child box) decides which children
+// to enter; on_particle(valid, i) is called by all lanes together for the particles of every
+// entered leaf (valid false on padding lanes) and returns false to abort. Returns false on abort
+// or stack overflow.
+template <class BoxTest, class OnParticle>
+__device__ bool warp_traverse(const SceneView& s, uint32_t* stk, uint32_t* leafbuf, uint32_t* status,
+                              BoxTest&& box_test, OnParticle&& on_particle) {
+  const uint32_t lane = threadIdx.x & 31u, lt = lane_lt_mask();
+  if (s.nleaves == 0) return true;
+  const uint32_t ppl = s.ppl;
+  if (s.root & kLeafBit) {
+    for (uint32_t b = 0; b < ppl; b += 32) {
+      uint32_t j = b + lane;
+      bool v = j < ppl && (uint64_t)j < s.n;
+      if (!on_particle(v, j)) return false;
+    }
+    return true;
+  }
+  if (lane == 0) stk[0] = s.root;
+  int sp = 1;
+  __syncwarp();
+  for (int guard = 0; sp > 0 && guard < (1 << 24); ++guard) {
+    const int take = sp < 32 ? sp : 32;
+    const int base = sp - take;
+    const bool valid = (int)lane < take;
+    uint32_t node = valid ? stk[base + lane] : 0u;
+    __syncwarp();
+    sp = base;
+    bool h0 = false, h1 = false;
+    uint2 ch = make_uint2(0u, 0u);
+    if (valid) {
+      const Node* nd = s.nodes + node;
+      float4 a = __ldg(&nd->a), b = __ldg(&nd->b), c = __ldg(&nd->c);
+      ch = __ldg(reinterpret_cast<const uint2*>(&nd->d));
+      h0 = box_test(a.x, a.y, a.z, a.w, b.x, b.y);
+      h1 = box_test(b.z, b.w, c.x, c.y, c.z, c.w);
+    }
+    const bool i0 = h0 && !(ch.x & kLeafBit), i1 = h1 && !(ch.y & kLeafBit);
+    const bool l0 = h0 && (ch.x & kLeafBit), l1 = h1 && (ch.y & kLeafBit);
+    const uint32_t m0 = __ballot_sync(kFull, i0), m1 = __ballot_sync(kFull, i1);
+    const int n0 = __popc(m0), n1 = __popc(m1);
+    if (sp + n0 + n1 > kWarpStack) {
+      if (lane == 0) atomicOr(status, kStatusStackOverflow);
+      return false;
+    }
+    if (i0) stk[sp + __popc(m0 & lt)] = ch.x;
+    if (i1) stk[sp + n0 + __popc(m1 & lt)] = ch.y;
+    sp += n0 + n1;
+    const uint32_t q0 = __ballot_sync(kFull, l0), q1 = __ballot_sync(kFull, l1);
+    const int c0 = __popc(q0), nl = c0 + __popc(q1);
+    if (l0) leafbuf[__popc(q0 & lt)] = ch.x & ~kLeafBit;
+    if (l1) leafbuf[c0 + __popc(q1 & lt)] = ch.y & ~kLeafBit;
+    __syncwarp();
+    const uint32_t total = (uint32_t)nl * ppl;
+    for (uint32_t b = 0; b < total; b += 32) {
+      uint32_t j = b + lane;
+      bool v = j < total;
+      uint64_t i = 0;
+      if (v) {
+        uint32_t leaf = leafbuf[j / ppl];
+        i = (uint64_t)leaf * ppl + (j % ppl);
+        v = i < s.n;
+      }
+      if (!on_particle(v, (uint32_t)i)) return false;
+    }
+    __syncwarp();
+  }
+  return true;
+}
+
+struct WarpStager {
+  WarpBuf* buf;
+  uint32_t* stk;
+  int ncand;
+  float rb_enter, rb_exit;
+  float3 inv;
+
+  __device__ void init(const SceneView& s, const Ray& ray) {
+    ncand = 0;
+    inv = make_float3(1.0f / ray.d.x, 1.0f / ray.d.y, 1.0f / ray.d.z);
+    float e = s.eps * 4.0f;
+    float ax = (s.root_lo[0] - e - ray.o.x) * inv.x, bx = (s.root_hi[0] + e - ray.o.x) * inv.x;
+    float ay = (s.root_lo[1] - e - ray.o.y) * inv.y, by = (s.root_hi[1] + e - ray.o.y) * inv.y;
+    float az = (s.root_lo[2] - e - ray.o.z) * inv.z, bz = (s.root_hi[2] + e - ray.o.z) * inv.z;
+    rb_enter = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz));
+    rb_exit = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
+    if (s.nleaves == 0 || !(rb_enter <= rb_exit)) {
+      rb_enter = __int_as_float(0x7f800000);
+      rb_exit = -__int_as_float(0x7f800000);
+    }
+  }
+
+  // stage every particle whose (slightly inflated) sphere meets [t0, t1]; false on overflow
+  __device__ bool stage(const SceneView& s, const Ray& ray, float t0, float t1, uint32_t* status) {
+    const uint32_t lt = lane_lt_mask();
+    const float eps = s.eps;
+    int n = 0;
+    bool ok = warp_traverse(
+        s, stk, buf->leaves, status,
+        [&](float lx, float ly, float lz, float hx, float hy, float hz) {
+          return seg_box(lx, ly, lz, hx, hy, hz, ray.o, inv, t0, t1, eps);
+        },
+        [&](bool v, uint32_t i) -> bool {
+          bool keep = false;
+          float a = 0.0f, b = 0.0f;
+          if (v) {
+            float4 r = __ldg(s.rec0 + i);
+            if (r.w > 0.0f) {
+              float vx = r.x - ray.o.x, vy = r.y - ray.o.y, vz = r.z - ray.o.z;
+              float tc = (vx * ray.d.x + vy * ray.d.y) + vz * ray.d.z;
+              float wx = vx - tc * ray.d.x, wy = vy - tc * ray.d.y, wz = vz - tc * ray.d.z;
+              float h2 = (wx * wx + wy * wy) + wz * wz;
+              float R = r.w * (1.0f + 0x1p-10f) + eps;
+              float R2 = R * R;
+              if (!(h2 > R2)) {
+                float half = sqrtf(R2 - h2) + eps;
+                a = tc - half;
+                b = tc + half;
+                keep = !(b < t0 || a > t1);
+              }
+            }
+          }
+          const uint32_t m = __ballot_sync(kFull, keep);
+          const int cnt = __popc(m);
+          if (n + cnt > kWarpCap) return false;
+          if (keep) {
+            int p = n + __popc(m & lt);
+            buf->idx[p] = i;
+            buf->lo[p] = a;
+            buf->hi[p] = b;
+          }
+          n += cnt;
+          return true;
+        });
+    __syncwarp();
+    ncand = ok ? n : 0;
+    return ok;
+  }
+
+  __device__ long long bin_sum(const SceneView& s, const Ray& ray, float lo, float hi) const {
+    long long acc = 0;
+    for (int j = (int)(threadIdx.x & 31u); j < ncand; j += 32) {
+      if (buf->hi[j] < lo || buf->lo[j] > hi) continue;
+      acc += fix40(bin_contrib(s, ray, buf->idx[j], lo, hi));
+    }
+    return warp_sum(acc);
+  }
+
+  __device__ void sample(const SceneView& s, float t, float3 x, Sample& acc) const {
+    sample_clear(acc);
+    for (int j = (int)(threadIdx.x & 31u); j < ncand; j += 32) {
+      if (t < buf->lo[j] || t > buf->hi[j]) continue;
+      eval_particle(s, buf->idx[j], x, acc);
+    }
+    warp_sum_sample(acc);
+  }
+
+  __device__ float lo_min() const {
+    float m = __int_as_float(0x7f800000);
+    for (int j = (int)(threadIdx.x & 31u); j < ncand; j += 32) m = fminf(m, buf->lo[j]);
+    return warp_min(m);
+  }
+
+  // direct (unbuffered) majorant sum of one bin
+  __device__ long long bin_sum_direct(const SceneView& s, const Ray& ray, float lo, float hi, uint32_t* status) {
+    long long acc = 0;
+    const float eps = s.eps;
+    warp_traverse(
+        s, stk, buf->leaves, status,
+        [&](float lx, float ly, float lz, float hx, float hy, float hz) {
+          return seg_box(lx, ly, lz, hx, hy, hz, ray.o, inv, lo, hi, eps);
+        },
+        [&](bool v, uint32_t i) -> bool {
+          if (v) acc += fix40(bin_contrib(s, ray, i, lo, hi));
+          return true;
+        });
+    return warp_sum(acc);
+  }
+
+  // direct point query
+  __device__ void point(const SceneView& s, float3 x, Sample& acc, uint32_t* status) {
+    sample_clear(acc);
+    warp_traverse(
+        s, stk, buf->leaves, status,
+        [&](float lx, float ly, float lz, float hx, float hy, float hz) { return inside(lx, ly, lz, hx, hy, hz, x); },
+        [&](bool v, uint32_t i) -> bool {
+          if (v) eval_particle(s, i, x, acc);
+          return true;
+        });
+    warp_sum_sample(acc);
+  }
+};
+
+// track_majorant with the warp-cooperative stager; same decisions, same random-number stream
+__device__ void track_majorant_warp(const RenderLaunch& L, Tracker& tr, const Ray& ray, WarpBuf* buf, uint32_t* stk) {
+  WarpStager st;
+  st.buf = buf;
+  st.stk = stk;
+  st.init(L.s, ray);
+  const float Lb = L.bin_length;
+  const float scale = L.density_scale;
+  const float minf = scale * 1.0078125f;
+  const float t0 = tr.t;
+  int k = 0;
+  float t = t0;
+  int seg_end = 0;
+  int nb = 32;
+  bool direct = false;
+  for (int guard = 0; guard < (1 << 26); ++guard) {
+    float b0 = t0 + (float)k * Lb;
+    float b1 = t0 + (float)(k + 1) * Lb;
+    if (!(b0 < ray.tmax) || !(b1 > b0)) break;
+    if (k >= seg_end) {
+      if (b1 < st.rb_enter) {
+        int ks = (int)floorf((st.rb_enter - t0) / Lb) - 1;
+        if (ks > k) {
+          k = ks;
+          t = t0 + (float)k * Lb;
+          continue;
+        }
+      }
+      if (b0 > st.rb_exit) break;
+      direct = false;
+      for (;;) {
+        float te = t0 + (float)(k + nb) * Lb;
+        if (st.stage(L.s, ray, b0, te, L.status)) {
+          seg_end = k + nb;
+          if (nb < 64) nb *= 2;
+          break;
+        }
+        nb >>= 1;
+        if (nb == 0) {
+          direct = true;
+          seg_end = k + 1;
+          nb = 1;
+          break;
+        }
+      }
+      if (!direct) {
+        if (st.ncand == 0) {
+          k = seg_end;
+          t = t0 + (float)k * Lb;
+          continue;
+        }
+        int ks = (int)floorf((st.lo_min() - t0) / Lb) - 1;
+        if (ks > k && ks < seg_end) {
+          k = ks;
+          t = t0 + (float)k * Lb;
+          continue;
+        }
+      }
+    }
+    float lo = b0, hi = b1;
+    int depth = 0, np = 0;
+    float pend_hi[kSplitDepth];
+    int pend_depth[kSplitDepth];
+    for (;;) {
+      long long acc = direct ? st.bin_sum_direct(L.s, ray, lo, hi, L.status) : st.bin_sum(L.s, ray, lo, hi);
+      float M = ((float)acc * kFixInv) * minf;
+      if (M > 0.0f) {
+        float mid = lo + 0.5f * (hi - lo);
+        if (M * (hi - lo) > kSplitSteps && depth < kSplitDepth && mid > lo && mid < hi) {
+          pend_hi[np] = hi;
+          pend_depth[np] = depth + 1;
+          ++np;
+          hi = mid;
+          depth += 1;
+          continue;
+        }
+        t = lo;
+        for (;;) {
+          if (tr.i >= kMaxDepth) {
+            tr.t = t;
+            return;
+          }
+          tr.i += 1;
+          float u = lcg_f(tr.rng);
+          float step = -dlog(1.0f - u) / M;
+          t = t + step;
+          if (t >= hi || t >= ray.tmax) break;
+          float3 x = make_float3(ray.o.x + t * ray.d.x, ray.o.y + t * ray.d.y, ray.o.z + t * ray.d.z);
+          Sample smp;
+          if (direct) st.point(L.s, x, smp, L.status);
+          else st.sample(L.s, t, x, smp);
+          float D = (float)smp.a0 * kFixInv;
+          float sigma = D * scale;
+          if (lcg_f(tr.rng) < sigma / M) {
+            float3 c = sample_color(L, smp, D);
+            tr.albedo = make_float4(c.x, c.y, c.z, 1.0f);
+            tr.t = t;
+            return;
+          }
+        }
+      }
+      if (np == 0) break;
+      lo = hi;
+      --np;
+      hi = pend_hi[np];
+      depth = pend_depth[np];
+    }
+    k += 1;
+    t = b1;
+  }
+  tr.t = t;
+}
+
+// persistent warps; an item is one sample of one pixel, ordered as in k_render
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render_warp(const RenderLaunch L) {
+  extern __shared__ __align__(16) char smem[];
+  const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+  WarpBuf* buf = reinterpret_cast<WarpBuf*>(smem) + wib;
+  uint32_t* stk = L.warp_stacks + ((size_t)blockIdx.x * kWarpsPerBlock + wib) * kWarpStack;
+  const uint32_t tiles_x = (uint32_t)(L.width + 7) / 8u;
+  const uint32_t spp = L.spp ? L.spp : 1u;
+  const uint32_t total = tiles_x * ((uint32_t)(L.height + 3) / 4u) * 32u * spp;
+  const size_t plane = (size_t)L.width * (size_t)L.height;
+  const bool cost = (L.flags & kFlagCostImage) != 0;
+  for (;;) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(L.work_counter, 1u);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= total) break;
+    uint32_t group = item >> 5, in = item & 31u;
+    uint32_t tile = group / spp, k = group % spp;
+    const int px = (int)((tile % tiles_x) * 8u + (in & 7u));
+    const int py = (int)((tile / tiles_x) * 4u + (in >> 3));
+    if (px >= L.width || py >= L.height) continue;
+    const size_t ofs = (size_t)px + (size_t)L.width * (size_t)py;
+    const long long c0 = cost ? clock64() : 0;
+    float noise = 0.0f;
+    float4 c = raygen_generic(L, (L.frame_id + k) & 0xffffu, px, py, noise, lane == 0,
+                              [&](Tracker& tr, const Ray& r, bool) { track_majorant_warp(L, tr, r, buf, stk); });
+    if (cost) c.w = (float)(clock64() - c0);
+    if (lane == 0) {
+      L.samples[(size_t)k * plane + ofs] = c;
+      if (k + 1 == spp) L.noise_buf[ofs] = noise;
+    }
+  }
 }
 
 // Persistent kernel: each thread repeatedly takes the next work item from a global counter.
@@ -853,8 +1254,53 @@ cudaError_t launch_cap(const RenderLaunch& L, cudaStream_t st) {
 
 }  // namespace
 
+namespace {
+
+cudaError_t warp_grid(int* blocks) {
+  static int cached = 0;
+  if (!cached) {
+    const size_t smem = sizeof(WarpBuf) * kWarpsPerBlock;
+    cudaError_t e = cudaFuncSetAttribute(k_render_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_warp, kWarpsPerBlock * 32, smem);
+    if (e != cudaSuccess) return e;
+    cached = sms * (per_sm > 0 ? per_sm : 1);
+  }
+  *blocks = cached;
+  return cudaSuccess;
+}
+
+}  // namespace
+
+bool render_uses_warp_kernel(const RenderLaunch& L) {
+  return L.traversal == AARBF_TRAVERSAL_AUTO && (L.flags & kFlagMajorantTracking) && !(L.flags & kFlagBlueNoise);
+}
+
+cudaError_t render_warp_stack_words(size_t* words) {
+  int blocks = 0;
+  cudaError_t e = warp_grid(&blocks);
+  *words = (size_t)blocks * kWarpsPerBlock * kWarpStack;
+  return e;
+}
+
 cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st) {
   if (L.width <= 0 || L.height <= 0) return cudaSuccess;
+  if (render_uses_warp_kernel(L)) {
+    int blocks = 0;
+    cudaError_t e = warp_grid(&blocks);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(L.work_counter, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    k_render_warp<<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf) * kWarpsPerBlock, st>>>(L);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    size_t plane = (size_t)L.width * (size_t)L.height;
+    k_accumulate<<<(unsigned)((plane + 255) / 256), 256, 0, st>>>(L);
+    return cudaGetLastError();
+  }
   switch (L.candidate_cap) {
     case 16: return launch_cap<16>(L, st);
     case 64: return launch_cap<64>(L, st);

@@ -57,10 +57,12 @@ enum {
                                                  pixel's samples took */
 };
 
-/* Traversal strategies of the render kernel (identical results). */
+/* Traversal strategies of the render kernel; every choice gives bit-identical results. */
 enum {
-  AARBF_TRAVERSAL_STAGED = 0, /* per-ray segments: candidates staged in shared memory */
-  AARBF_TRAVERSAL_POINT = 1   /* one BVH point query per tracking step (reference shape) */
+  AARBF_TRAVERSAL_AUTO = 0,  /* majorant tracking: one warp per ray (cooperative traversal and
+                                sums); otherwise per-thread staged segments */
+  AARBF_TRAVERSAL_POINT = 1, /* one BVH point query per tracking step (reference shape) */
+  AARBF_TRAVERSAL_THREAD = 2 /* per-thread staged segments for every estimator */
 };
 
 /*

@@ -229,7 +229,8 @@ def test_render_native_mode(ctx, orc, aarbf_mod, traversal):
 @pytest.mark.parametrize("n,ppl,bins,scale,floor", [(30_000, 1, 4.0, 200.0, 0.0), (30_000, 4, 1.0, 200.0, 0.0),
                                                     (200_000, 1, 8.0, 200.0, 1 / 255),
                                                     (200_000, 8, 32.0, 5000.0, 1 / 255)])
-def test_render_majorant_tracking(ctx, orc, aarbf_mod, n, ppl, bins, scale, floor):
+@pytest.mark.parametrize("traversal", [0, 2])  # one warp per ray / one thread per ray
+def test_render_majorant_tracking(ctx, orc, aarbf_mod, n, ppl, bins, scale, floor, traversal):
     """delta tracking with per-bin majorants (native extinction density_scale * D); the dense
     case exercises the bin refinement and the direct (unstaged) bins"""
     from aarbf import scenes
@@ -238,7 +239,7 @@ def test_render_majorant_tracking(ctx, orc, aarbf_mod, n, ppl, bins, scale, floo
     dom = orc.domain([sc.xyzw])
     w, h = 40, 30
     rp = scenes.native_params(scenes.orbit_camera(), w, h, float(sc.radii.max()), 0.002, scale, dom, spp=2,
-                              majorant=True, bin_length=bins * 0.002)
+                              majorant=True, bin_length=bins * 0.002, traversal=traversal)
     scene, *_ = setup_both(ctx, orc, aarbf_mod, sc.xyzw, sc.radii, ppl, rp.rbf_radius, tf32=(cm, rm, dm),
                            alpha_floor=floor)
     ga, gi = gpu_render(ctx, rp, w, h)
