@@ -78,7 +78,7 @@ class Params(ctypes.Structure):
         ("aabb_min", ctypes.c_float * 3), ("aabb_max", ctypes.c_float * 3),
         ("density_gain", ctypes.c_float), ("jitter_x", ctypes.c_float), ("jitter_y", ctypes.c_float),
         ("traversal", ctypes.c_int32), ("density_scale", ctypes.c_float), ("bin_length", ctypes.c_float),
-        ("candidate_cap", ctypes.c_int32),
+        ("candidate_cap", ctypes.c_int32), ("stage_bins", ctypes.c_int32),
     ]
 
 
@@ -261,6 +261,7 @@ class RenderParams:
     density_scale: float = 0.0
     bin_length: float = 0.0
     candidate_cap: int = 0
+    stage_bins: int = 0
 
     def to_c(self) -> Params:
         p = Params()
@@ -275,6 +276,7 @@ class RenderParams:
         p.traversal = int(self.traversal)
         p.density_scale, p.bin_length = self.density_scale, self.bin_length
         p.candidate_cap = int(self.candidate_cap)
+        p.stage_bins = int(self.stage_bins)
         return p
 
 

@@ -74,6 +74,7 @@ struct RenderLaunch {
   float density_scale, bin_length; // majorant tracking
   uint32_t* work_counter;          // persistent kernel: next pixel tile item (zeroed per launch)
   int candidate_cap;               // staging buffer depth per ray (template instance)
+  int stage_bins;                  // majorant tracking: bins staged first (1..64)
   float4* samples;                 // spp planes of per-sample colours (width * height each)
   float* noise_buf;                // per pixel: noise value of the last sample (showNoise)
   uint32_t* warp_stacks;           // ray-per-warp kernel: one traversal stack per resident warp

@@ -214,9 +214,22 @@ aarbf_status fill_launch(aarbf_ctx* ctx, const aarbf_params* p, int w, int h, fl
   L.splat_rmax = (p->flags & kFlagSplatParticleRadius) ? ctx->max_radius : p->rbf_radius;
   L.density_scale = p->density_scale;
   L.bin_length = p->bin_length;
-  L.candidate_cap = p->candidate_cap ? p->candidate_cap : 32;
-  if (L.candidate_cap != 16 && L.candidate_cap != 32 && L.candidate_cap != 64 && L.candidate_cap != 128)
-    return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "candidate_cap must be 16, 32, 64 or 128");
+  L.stage_bins = p->stage_bins;
+  if (L.stage_bins < 0 || L.stage_bins > 64)
+    return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "stage_bins must lie in 1..64 (0 = default)");
+  L.candidate_cap = p->candidate_cap;
+  {
+    const bool warp = render_uses_warp_kernel(L);
+    const int c = p->candidate_cap;
+    if (L.stage_bins == 0) L.stage_bins = warp ? 4 : 16;
+    if (c == 0) {
+      L.candidate_cap = warp ? 256 : 32;
+    } else if (warp ? (c != 256 && c != 512 && c != 1024) : (c != 16 && c != 32 && c != 64 && c != 128)) {
+      return fail(ctx, AARBF_ERR_INVALID_ARGUMENT,
+                  warp ? "candidate_cap must be 256, 512 or 1024 for the warp kernel"
+                       : "candidate_cap must be 16, 32, 64 or 128");
+    }
+  }
   if (!(p->unit > 0.0f)) return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "unit must be > 0");
   if ((p->flags & kFlagMajorantTracking) && !(p->bin_length > 0.0f && p->density_scale >= 0.0f))
     return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "majorant tracking needs bin_length > 0, density_scale >= 0");

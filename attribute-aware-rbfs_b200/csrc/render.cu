@@ -377,7 +377,8 @@ __device__ __forceinline__ float sample_density(const RenderLaunch& L, float D) 
   return tex1(L.s.tf_density, L.s.nd, D);
 }
 
-__device__ __forceinline__ float3 sample_color(const RenderLaunch& L, const Sample& acc, float D) {
+// out of line: runs once per collision, and keeps three pow expansions out of the hot loops
+__device__ __noinline__ float3 sample_color(const RenderLaunch& L, const Sample& acc, float D) {
   if (L.flags & kFlagVisualizeAttributes) {
     const float g = 1.0f / 2.2f;
     float c0 = (float)acc.a1 * kFixInv, c1 = (float)acc.a2 * kFixInv, c2 = (float)acc.a3 * kFixInv;
@@ -548,7 +549,7 @@ __device__ void track_majorant(const RenderLaunch& L, Tracker& tr, const Ray& ra
   int k = 0;
   float t = t0;
   int seg_end = 0;   // bins below seg_end are covered by the staged candidates
-  int nb = 16;       // bins per staging
+  int nb = L.stage_bins;  // bins per staging
   bool direct = false;
   for (int guard = 0; guard < (1 << 26); ++guard) {
     float b0 = t0 + (float)k * Lb;
@@ -770,20 +771,24 @@ __device__ float4 raygen_sample(const RenderLaunch& L, uint32_t frame, int px, i
 // Ray-per-warp kernel for majorant tracking. All 32 lanes of a warp work on one ray: the
 // sequential tracker logic runs uniformly on every lane (identical values), and the heavy parts
 // are split across lanes -- BVH traversal as a warp-wide frontier compacted with ballots,
-// candidate staging into a per-warp shared buffer, and the fixed-point sums of majorants and
-// densities, which lanes accumulate over disjoint particles and combine with shuffles (integer
-// sums, so the lane split cannot change a bit).
+// candidate staging into a per-warp shared buffer bucketed by majorant bin, and the fixed-point
+// sums of majorants and densities, which lanes accumulate over disjoint particles and combine
+// with shuffles (integer sums, so the lane split cannot change a bit).
 // ============================================================================================
 
-constexpr int kWarpCap = 1024;        // staged candidates per ray (per warp)
 constexpr int kWarpsPerBlock = 4;
 constexpr int kWarpStack = 8192;      // traversal stack entries per warp (global memory)
+constexpr int kMaxSegBins = 64;       // bins per staged segment
 constexpr unsigned kFull = 0xffffffffu;
 
+// per-warp shared memory: staged candidates, then per-bin lists of candidate slots (CSR)
+template <int CAPW>
 struct WarpBuf {
-  uint32_t idx[kWarpCap];
-  float lo[kWarpCap];
-  float hi[kWarpCap];
+  uint32_t idx[CAPW];
+  float lo[CAPW];
+  float hi[CAPW];
+  uint16_t list[2 * CAPW];
+  uint32_t start[kMaxSegBins + 1];
   uint32_t leaves[64];
 };
 
@@ -805,12 +810,6 @@ __device__ __forceinline__ int warp_sum(int v) {
   return v;
 }
 
-__device__ __forceinline__ float warp_min(float v) {
-#pragma unroll
-  for (int o = 16; o; o >>= 1) v = fminf(v, __shfl_xor_sync(kFull, v, o));
-  return v;
-}
-
 __device__ __forceinline__ void warp_sum_sample(Sample& s) {
   s.count = warp_sum(s.count);
   s.a0 = warp_sum(s.a0);
@@ -823,9 +822,17 @@ __device__ __forceinline__ void warp_sum_sample(Sample& s) {
 // to enter; on_particle(valid, i) is called by all lanes together for the particles of every
 // entered leaf (valid false on padding lanes) and returns false to abort. Returns false on abort
 // or stack overflow.
+// warp-kernel count-mode slots (lane 0 adds warp-uniform values)
+enum { kWcSteps = 2, kWcStages = 3, kWcOverflows = 4, kWcDirect = 5, kWcCands = 6, kWcBins = 7,
+       kWcIters = 8, kWcParticles = 9 };
+
+__device__ __forceinline__ void wctr(unsigned long long* c, int i, unsigned long long v) {
+  if (c && (threadIdx.x & 31u) == 0) atomicAdd(c + i, v);
+}
+
 template <class BoxTest, class OnParticle>
 __device__ bool warp_traverse(const SceneView& s, uint32_t* stk, uint32_t* leafbuf, uint32_t* status,
-                              BoxTest&& box_test, OnParticle&& on_particle) {
+                              BoxTest&& box_test, OnParticle&& on_particle, unsigned long long* ctr = nullptr) {
   const uint32_t lane = threadIdx.x & 31u, lt = lane_lt_mask();
   if (s.nleaves == 0) return true;
   const uint32_t ppl = s.ppl;
@@ -873,6 +880,8 @@ __device__ bool warp_traverse(const SceneView& s, uint32_t* stk, uint32_t* leafb
     if (l1) leafbuf[c0 + __popc(q1 & lt)] = ch.y & ~kLeafBit;
     __syncwarp();
     const uint32_t total = (uint32_t)nl * ppl;
+    wctr(ctr, kWcIters, 1);
+    wctr(ctr, kWcParticles, total);
     for (uint32_t b = 0; b < total; b += 32) {
       uint32_t j = b + lane;
       bool v = j < total;
@@ -889,15 +898,22 @@ __device__ bool warp_traverse(const SceneView& s, uint32_t* stk, uint32_t* leafb
   return true;
 }
 
+template <int CAPW>
 struct WarpStager {
-  WarpBuf* buf;
+  WarpBuf<CAPW>* buf;
   uint32_t* stk;
   int ncand;
+  int kseg, nbins;   // the staged segment covers bins [kseg, kseg + nbins)
+  bool lists;        // per-bin lists are valid
   float rb_enter, rb_exit;
   float3 inv;
+  unsigned long long* ctr;
 
   __device__ void init(const SceneView& s, const Ray& ray) {
     ncand = 0;
+    kseg = 0;
+    nbins = 0;
+    lists = false;
     inv = make_float3(1.0f / ray.d.x, 1.0f / ray.d.y, 1.0f / ray.d.z);
     float e = s.eps * 4.0f;
     float ax = (s.root_lo[0] - e - ray.o.x) * inv.x, bx = (s.root_hi[0] + e - ray.o.x) * inv.x;
@@ -911,15 +927,28 @@ struct WarpStager {
     }
   }
 
-  // stage every particle whose (slightly inflated) sphere meets [t0, t1]; false on overflow
-  __device__ bool stage(const SceneView& s, const Ray& ray, float t0, float t1, uint32_t* status) {
-    const uint32_t lt = lane_lt_mask();
+  // conservative range of segment bins a candidate interval [a, b] may touch
+  __device__ __forceinline__ void bin_span(float a, float b, float t0, float Lb, int& j0, int& j1) const {
+    float fa = floorf((a - t0) / Lb), fb = floorf((b - t0) / Lb);
+    float lo = (float)(kseg - 1), hi = (float)(kseg + nbins);
+    fa = fminf(fmaxf(fa, lo), hi);
+    fb = fminf(fmaxf(fb, lo), hi);
+    j0 = max((int)fa - 1 - kseg, 0);
+    j1 = min((int)fb + 1 - kseg, nbins - 1);
+  }
+
+  // stage every particle whose (slightly inflated) sphere meets bins [k, k + nb) and bucket the
+  // candidates by bin; false on overflow
+  __device__ bool stage(const SceneView& s, const Ray& ray, int k, int nb, float t0, float Lb, uint32_t* status) {
+    const uint32_t lane = threadIdx.x & 31u, lt = lane_lt_mask();
+    wctr(ctr, kWcStages, 1);
     const float eps = s.eps;
+    const float ts = t0 + (float)k * Lb, te = t0 + (float)(k + nb) * Lb;
     int n = 0;
     bool ok = warp_traverse(
         s, stk, buf->leaves, status,
         [&](float lx, float ly, float lz, float hx, float hy, float hz) {
-          return seg_box(lx, ly, lz, hx, hy, hz, ray.o, inv, t0, t1, eps);
+          return seg_box(lx, ly, lz, hx, hy, hz, ray.o, inv, ts, te, eps);
         },
         [&](bool v, uint32_t i) -> bool {
           bool keep = false;
@@ -937,13 +966,13 @@ struct WarpStager {
                 float half = sqrtf(R2 - h2) + eps;
                 a = tc - half;
                 b = tc + half;
-                keep = !(b < t0 || a > t1);
+                keep = !(b < ts || a > te);
               }
             }
           }
           const uint32_t m = __ballot_sync(kFull, keep);
           const int cnt = __popc(m);
-          if (n + cnt > kWarpCap) return false;
+          if (n + cnt > CAPW) return false;
           if (keep) {
             int p = n + __popc(m & lt);
             buf->idx[p] = i;
@@ -952,38 +981,116 @@ struct WarpStager {
           }
           n += cnt;
           return true;
-        });
+        },
+        ctr);
     __syncwarp();
-    ncand = ok ? n : 0;
-    return ok;
+    if (!ok) {
+      wctr(ctr, kWcOverflows, 1);
+      ncand = 0;
+      return false;
+    }
+    wctr(ctr, kWcCands, n);
+    ncand = n;
+    kseg = k;
+    nbins = nb;
+    // per-bin lists: count, exclusive scan, fill
+    for (int j = (int)lane; j <= nb; j += 32) buf->start[j] = 0u;
+    __syncwarp();
+    for (int c = (int)lane; c < n; c += 32) {
+      int j0, j1;
+      bin_span(buf->lo[c], buf->hi[c], t0, Lb, j0, j1);
+      for (int j = j0; j <= j1; ++j) atomicAdd(&buf->start[j + 1], 1u);
+    }
+    __syncwarp();
+    uint32_t c0 = lane < (uint32_t)nb ? buf->start[lane + 1] : 0u;
+    uint32_t c1 = lane + 32u < (uint32_t)nb ? buf->start[lane + 33] : 0u;
+    uint32_t x0 = c0, x1 = c1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y0 = __shfl_up_sync(kFull, x0, o), y1 = __shfl_up_sync(kFull, x1, o);
+      if ((int)lane >= o) {
+        x0 += y0;
+        x1 += y1;
+      }
+    }
+    const uint32_t tot0 = __shfl_sync(kFull, x0, 31);
+    const uint32_t total = tot0 + __shfl_sync(kFull, x1, 31);
+    __syncwarp();
+    // start[j] = first slot of bin j (exclusive prefix); start[nb] = total
+    if (lane < (uint32_t)nb) buf->start[lane] = x0 - c0;
+    if (lane + 32u < (uint32_t)nb) buf->start[lane + 32] = tot0 + x1 - c1;
+    if (lane == 0) buf->start[nb] = total;
+    lists = total <= 2u * CAPW;
+    __syncwarp();
+    if (lists) {
+      // fill with per-bin cursors kept in the upper half of list[] scratch: reuse start[] by
+      // counting down from the bin end
+      uint32_t* cur = buf->leaves;  // 64 cursors (nb <= 64)
+      for (int j = (int)lane; j < nb; j += 32) cur[j] = buf->start[j];
+      __syncwarp();
+      for (int c = (int)lane; c < n; c += 32) {
+        int j0, j1;
+        bin_span(buf->lo[c], buf->hi[c], t0, Lb, j0, j1);
+        for (int j = j0; j <= j1; ++j) buf->list[atomicAdd(&cur[j], 1u)] = (uint16_t)c;
+      }
+      __syncwarp();
+    }
+    return true;
   }
 
-  __device__ long long bin_sum(const SceneView& s, const Ray& ray, float lo, float hi) const {
+  // candidate slots for top-level bin kbin: [first, last) in list[] (or all candidates)
+  __device__ __forceinline__ void range(int kbin, int& first, int& last) const {
+    if (lists) {
+      int j = kbin - kseg;
+      first = (int)buf->start[j];
+      last = (int)buf->start[j + 1];
+    } else {
+      first = 0;
+      last = ncand;
+    }
+  }
+
+  __device__ __forceinline__ int slot(int p) const { return lists ? (int)buf->list[p] : p; }
+
+  __device__ long long bin_sum(const SceneView& s, const Ray& ray, int kbin, float lo, float hi) const {
+    int first, last;
+    range(kbin, first, last);
     long long acc = 0;
-    for (int j = (int)(threadIdx.x & 31u); j < ncand; j += 32) {
+    for (int p = first + (int)(threadIdx.x & 31u); p < last; p += 32) {
+      int j = slot(p);
       if (buf->hi[j] < lo || buf->lo[j] > hi) continue;
       acc += fix40(bin_contrib(s, ray, buf->idx[j], lo, hi));
     }
     return warp_sum(acc);
   }
 
-  __device__ void sample(const SceneView& s, float t, float3 x, Sample& acc) const {
+  __device__ void sample(const SceneView& s, int kbin, float t, float3 x, Sample& acc) const {
+    int first, last;
+    range(kbin, first, last);
     sample_clear(acc);
-    for (int j = (int)(threadIdx.x & 31u); j < ncand; j += 32) {
+    for (int p = first + (int)(threadIdx.x & 31u); p < last; p += 32) {
+      int j = slot(p);
       if (t < buf->lo[j] || t > buf->hi[j]) continue;
       eval_particle(s, buf->idx[j], x, acc);
     }
     warp_sum_sample(acc);
   }
 
-  __device__ float lo_min() const {
-    float m = __int_as_float(0x7f800000);
-    for (int j = (int)(threadIdx.x & 31u); j < ncand; j += 32) m = fminf(m, buf->lo[j]);
-    return warp_min(m);
+  // first bin >= k of the staged segment whose list is not empty (kseg + nbins if none)
+  __device__ int next_nonempty(int k) const {
+    if (!lists) return k;
+    for (int j = k - kseg; j < nbins; j += 32) {
+      int jj = j + (int)(threadIdx.x & 31u);
+      bool ne = jj < nbins && buf->start[jj + 1] > buf->start[jj];
+      uint32_t m = __ballot_sync(kFull, ne);
+      if (m) return kseg + j + __ffs(m) - 1;
+    }
+    return kseg + nbins;
   }
 
   // direct (unbuffered) majorant sum of one bin
-  __device__ long long bin_sum_direct(const SceneView& s, const Ray& ray, float lo, float hi, uint32_t* status) {
+  __device__ __noinline__ long long bin_sum_direct(const SceneView& s, const Ray& ray, float lo, float hi,
+                                                 uint32_t* status) {
     long long acc = 0;
     const float eps = s.eps;
     warp_traverse(
@@ -994,12 +1101,14 @@ struct WarpStager {
         [&](bool v, uint32_t i) -> bool {
           if (v) acc += fix40(bin_contrib(s, ray, i, lo, hi));
           return true;
-        });
+        },
+        ctr);
+    wctr(ctr, kWcDirect, 1);
     return warp_sum(acc);
   }
 
   // direct point query
-  __device__ void point(const SceneView& s, float3 x, Sample& acc, uint32_t* status) {
+  __device__ __noinline__ void point(const SceneView& s, float3 x, Sample& acc, uint32_t* status) {
     sample_clear(acc);
     warp_traverse(
         s, stk, buf->leaves, status,
@@ -1007,16 +1116,22 @@ struct WarpStager {
         [&](bool v, uint32_t i) -> bool {
           if (v) eval_particle(s, i, x, acc);
           return true;
-        });
+        },
+        ctr);
+    wctr(ctr, kWcDirect, 1);
     warp_sum_sample(acc);
   }
 };
 
 // track_majorant with the warp-cooperative stager; same decisions, same random-number stream
-__device__ void track_majorant_warp(const RenderLaunch& L, Tracker& tr, const Ray& ray, WarpBuf* buf, uint32_t* stk) {
-  WarpStager st;
+// out of line: one copy serves the primary and the shadow ray (instruction-cache footprint)
+template <int CAPW>
+__device__ __noinline__ void track_majorant_warp(const RenderLaunch& L, Tracker& tr, const Ray& ray, WarpBuf<CAPW>* buf,
+                                    uint32_t* stk) {
+  WarpStager<CAPW> st;
   st.buf = buf;
   st.stk = stk;
+  st.ctr = L.counters;
   st.init(L.s, ray);
   const float Lb = L.bin_length;
   const float scale = L.density_scale;
@@ -1025,7 +1140,7 @@ __device__ void track_majorant_warp(const RenderLaunch& L, Tracker& tr, const Ra
   int k = 0;
   float t = t0;
   int seg_end = 0;
-  int nb = 32;
+  int nb = L.stage_bins;
   bool direct = false;
   for (int guard = 0; guard < (1 << 26); ++guard) {
     float b0 = t0 + (float)k * Lb;
@@ -1043,10 +1158,9 @@ __device__ void track_majorant_warp(const RenderLaunch& L, Tracker& tr, const Ra
       if (b0 > st.rb_exit) break;
       direct = false;
       for (;;) {
-        float te = t0 + (float)(k + nb) * Lb;
-        if (st.stage(L.s, ray, b0, te, L.status)) {
+        if (st.stage(L.s, ray, k, nb, t0, Lb, L.status)) {
           seg_end = k + nb;
-          if (nb < 64) nb *= 2;
+          if (nb < kMaxSegBins) nb *= 2;
           break;
         }
         nb >>= 1;
@@ -1063,12 +1177,15 @@ __device__ void track_majorant_warp(const RenderLaunch& L, Tracker& tr, const Ra
           t = t0 + (float)k * Lb;
           continue;
         }
-        int ks = (int)floorf((st.lo_min() - t0) / Lb) - 1;
-        if (ks > k && ks < seg_end) {
-          k = ks;
-          t = t0 + (float)k * Lb;
-          continue;
-        }
+      }
+    }
+    if (!direct) {
+      // bins whose candidate list is empty have majorant 0: skip them without drawing
+      int kn = st.next_nonempty(k);
+      if (kn > k) {
+        k = kn;
+        t = t0 + (float)k * Lb;
+        continue;
       }
     }
     float lo = b0, hi = b1;
@@ -1076,7 +1193,8 @@ __device__ void track_majorant_warp(const RenderLaunch& L, Tracker& tr, const Ra
     float pend_hi[kSplitDepth];
     int pend_depth[kSplitDepth];
     for (;;) {
-      long long acc = direct ? st.bin_sum_direct(L.s, ray, lo, hi, L.status) : st.bin_sum(L.s, ray, lo, hi);
+      wctr(L.counters, kWcBins, 1);
+      long long acc = direct ? st.bin_sum_direct(L.s, ray, lo, hi, L.status) : st.bin_sum(L.s, ray, k, lo, hi);
       float M = ((float)acc * kFixInv) * minf;
       if (M > 0.0f) {
         float mid = lo + 0.5f * (hi - lo);
@@ -1095,6 +1213,7 @@ __device__ void track_majorant_warp(const RenderLaunch& L, Tracker& tr, const Ra
             return;
           }
           tr.i += 1;
+          wctr(L.counters, kWcSteps, 1);
           float u = lcg_f(tr.rng);
           float step = -dlog(1.0f - u) / M;
           t = t + step;
@@ -1102,7 +1221,7 @@ __device__ void track_majorant_warp(const RenderLaunch& L, Tracker& tr, const Ra
           float3 x = make_float3(ray.o.x + t * ray.d.x, ray.o.y + t * ray.d.y, ray.o.z + t * ray.d.z);
           Sample smp;
           if (direct) st.point(L.s, x, smp, L.status);
-          else st.sample(L.s, t, x, smp);
+          else st.sample(L.s, k, t, x, smp);
           float D = (float)smp.a0 * kFixInv;
           float sigma = D * scale;
           if (lcg_f(tr.rng) < sigma / M) {
@@ -1126,10 +1245,11 @@ __device__ void track_majorant_warp(const RenderLaunch& L, Tracker& tr, const Ra
 }
 
 // persistent warps; an item is one sample of one pixel, ordered as in k_render
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render_warp(const RenderLaunch L) {
+template <int CAPW>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_render_warp(const RenderLaunch L) {
   extern __shared__ __align__(16) char smem[];
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
-  WarpBuf* buf = reinterpret_cast<WarpBuf*>(smem) + wib;
+  WarpBuf<CAPW>* buf = reinterpret_cast<WarpBuf<CAPW>*>(smem) + wib;
   uint32_t* stk = L.warp_stacks + ((size_t)blockIdx.x * kWarpsPerBlock + wib) * kWarpStack;
   const uint32_t tiles_x = (uint32_t)(L.width + 7) / 8u;
   const uint32_t spp = L.spp ? L.spp : 1u;
@@ -1150,7 +1270,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render_warp(const Rende
     const long long c0 = cost ? clock64() : 0;
     float noise = 0.0f;
     float4 c = raygen_generic(L, (L.frame_id + k) & 0xffffu, px, py, noise, lane == 0,
-                              [&](Tracker& tr, const Ray& r, bool) { track_majorant_warp(L, tr, r, buf, stk); });
+                              [&](Tracker& tr, const Ray& r, bool) { track_majorant_warp<CAPW>(L, tr, r, buf, stk); });
     if (cost) c.w = (float)(clock64() - c0);
     if (lane == 0) {
       L.samples[(size_t)k * plane + ofs] = c;
@@ -1256,21 +1376,38 @@ cudaError_t launch_cap(const RenderLaunch& L, cudaStream_t st) {
 
 namespace {
 
+template <int CAPW>
 cudaError_t warp_grid(int* blocks) {
   static int cached = 0;
   if (!cached) {
-    const size_t smem = sizeof(WarpBuf) * kWarpsPerBlock;
-    cudaError_t e = cudaFuncSetAttribute(k_render_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = sizeof(WarpBuf<CAPW>) * kWarpsPerBlock;
+    cudaError_t e =
+        cudaFuncSetAttribute(k_render_warp<CAPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_warp, kWarpsPerBlock * 32, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_warp<CAPW>, kWarpsPerBlock * 32, smem);
     if (e != cudaSuccess) return e;
     cached = sms * (per_sm > 0 ? per_sm : 1);
   }
   *blocks = cached;
   return cudaSuccess;
+}
+
+template <int CAPW>
+cudaError_t launch_warp(const RenderLaunch& L, cudaStream_t st) {
+  int blocks = 0;
+  cudaError_t e = warp_grid<CAPW>(&blocks);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(L.work_counter, 0, sizeof(uint32_t), st);
+  if (e != cudaSuccess) return e;
+  k_render_warp<CAPW><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  size_t plane = (size_t)L.width * (size_t)L.height;
+  k_accumulate<<<(unsigned)((plane + 255) / 256), 256, 0, st>>>(L);
+  return cudaGetLastError();
 }
 
 }  // namespace
@@ -1280,8 +1417,12 @@ bool render_uses_warp_kernel(const RenderLaunch& L) {
 }
 
 cudaError_t render_warp_stack_words(size_t* words) {
-  int blocks = 0;
-  cudaError_t e = warp_grid(&blocks);
+  // enough stacks for the largest grid of any buffer depth
+  int b0 = 0, b1 = 0, b2 = 0;
+  cudaError_t e = warp_grid<256>(&b0);
+  if (e == cudaSuccess) e = warp_grid<512>(&b1);
+  if (e == cudaSuccess) e = warp_grid<1024>(&b2);
+  int blocks = max(b0, max(b1, b2));
   *words = (size_t)blocks * kWarpsPerBlock * kWarpStack;
   return e;
 }
@@ -1289,17 +1430,11 @@ cudaError_t render_warp_stack_words(size_t* words) {
 cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st) {
   if (L.width <= 0 || L.height <= 0) return cudaSuccess;
   if (render_uses_warp_kernel(L)) {
-    int blocks = 0;
-    cudaError_t e = warp_grid(&blocks);
-    if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(L.work_counter, 0, sizeof(uint32_t), st);
-    if (e != cudaSuccess) return e;
-    k_render_warp<<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf) * kWarpsPerBlock, st>>>(L);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    size_t plane = (size_t)L.width * (size_t)L.height;
-    k_accumulate<<<(unsigned)((plane + 255) / 256), 256, 0, st>>>(L);
-    return cudaGetLastError();
+    switch (L.candidate_cap) {
+      case 512: return launch_warp<512>(L, st);
+      case 1024: return launch_warp<1024>(L, st);
+      default: return launch_warp<256>(L, st);
+    }
   }
   switch (L.candidate_cap) {
     case 16: return launch_cap<16>(L, st);

@@ -61,7 +61,8 @@ def parse():
     ap.add_argument("--bin", type=float, default=16.0, help="majorant bin length in units")
     ap.add_argument("--alpha-floor", type=float, default=1.0 / 255.0,
                     help="opacity below this is transparent (1/255: the 8-bit transfer-function resolution)")
-    ap.add_argument("--cap", type=int, default=32, help="staged candidates per ray (16/32/64/128)")
+    ap.add_argument("--cap", type=int, default=0,
+                    help="staged candidates per ray: 256/512/1024 per warp (majorant), 0 = default")
     ap.add_argument("--plain-spp", type=int, default=1, help="spp of the plain-estimator comparison (0: skip)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -168,7 +169,7 @@ def params_for(args, dom, rmax, frame_id=0, estimator=None, spp=None):
                               args.density_scale, dom, spp=spp or args.spp, frame_id=frame_id,
                               traversal=args.traversal, majorant=(est == "majorant"),
                               bin_length=args.bin * args.unit)
-    rp.candidate_cap = args.cap
+    rp.candidate_cap = args.cap if est == "majorant" else 0
     return rp
 
 
@@ -237,6 +238,16 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def traversal_label(args):
+    if args.traversal == 1:
+        return "point queries per step (thread per sample)"
+    if args.traversal == 2:
+        return "staged segments (thread per sample)"
+    if args.estimator == "majorant":
+        return "ray per warp (warp-wide BVH frontier, shared candidate lists)"
+    return "staged segments (thread per sample)"
+
+
 def config_dict(args):
     return {"workload": f"clusters_{args.particles // 1_000_000}M_{args.width}x{args.height}_{args.spp}spp_delta_tracking",
             "particles": args.particles, "width": args.width, "height": args.height, "spp": args.spp,
@@ -244,7 +255,7 @@ def config_dict(args):
                           if args.estimator == "majorant" else
                           "delta tracking with the global majorant 1/unit + shadow ray"),
             "unit": args.unit, "density_scale": args.density_scale,
-            "traversal": "staged" if args.traversal == 0 else "point", "particles_per_leaf": args.ppl,
+            "traversal": traversal_label(args), "particles_per_leaf": args.ppl,
             "alpha_floor": args.alpha_floor, "candidate_cap": args.cap,
             "l2": "inputs_larger_than_l2", "parallelism": f"replicas{args.gpus}"}
 

@@ -87,8 +87,12 @@ typedef struct aarbf_params {
   int32_t traversal;        /* AARBF_TRAVERSAL_* */
   float density_scale;      /* AARBF_FLAG_MAJORANT_TRACKING: extinction per unit length per unit D */
   float bin_length;         /* AARBF_FLAG_MAJORANT_TRACKING: majorant bin length along a ray */
-  int32_t candidate_cap;    /* staged candidates per ray: 16, 32, 64 or 128 (0 = 32); tuning only,
-                               results are identical for every value */
+  int32_t candidate_cap;    /* staged candidates per ray: 16, 32, 64 or 128 per thread (0 = 32),
+                               or 256, 512 or 1024 per warp for the warp kernel (0 = 256);
+                               tuning only, results are identical for every value */
+  int32_t stage_bins;       /* majorant tracking: bins staged by the first traversal of a ray
+                               (1..64; 0 = 4 for the warp kernel, 16 per thread; later stagings
+                               double up to 64); tuning only */
 } aarbf_params;
 
 /* ---- context -------------------------------------------------------------------------- */
