@@ -37,6 +37,12 @@ TRAVERSAL_STAGED = 0
 TRAVERSAL_POINT = 1     # one BVH point query per tracking step
 TRAVERSAL_THREAD = 2    # per-thread staged segments for every estimator
 
+
+def uses_warp_kernel(p) -> bool:
+    """True when a render with these parameters runs the ray-per-warp kernel."""
+    return (int(p.traversal) == TRAVERSAL_AUTO and bool(p.flags & FLAG_MAJORANT_TRACKING)
+            and not p.flags & FLAG_BLUE_NOISE)
+
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "out of memory", 3: "CUDA error",
     4: "device-side limit exceeded", 5: "not ready", 6: "I/O error", 7: "unsupported",
@@ -54,7 +60,7 @@ EXPORTED_SYMBOLS = (
     "aarbf_get_num_particles", "aarbf_get_hilbert_keys", "aarbf_get_sorted_particles",
     "aarbf_get_prepass", "aarbf_get_bvh", "aarbf_device_alloc", "aarbf_device_free",
     "aarbf_memcpy", "aarbf_memset", "aarbf_render_count", "aarbf_set_opacity_floor",
-    "aarbf_hilbert_sort_noalloc",
+    "aarbf_hilbert_sort_noalloc", "aarbf_set_kernel_timing", "aarbf_get_kernel_times",
 )
 
 
@@ -126,6 +132,9 @@ def _load():
         "aarbf_memcpy": [P, P, P, ctypes.c_size_t, P],
         "aarbf_memset": [P, P, i32, ctypes.c_size_t, P],
         "aarbf_render_count": [P, ctypes.POINTER(Params), i32, i32, P, P, P, P],
+        "aarbf_set_kernel_timing": [P, i32],
+        "aarbf_get_kernel_times": [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(u32)],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -378,9 +387,25 @@ class Context:
         c = np.zeros(10, np.uint64)
         self._check(self._lib.aarbf_render_count(self._h, ctypes.byref(p), int(width), int(height),
                                                  _ptr(accum), _ptr(image), _ptr(c), _stream_ptr(stream)))
-        names = ("segment_particles", "segment_nodes", "steps", "stagings", "staging_overflows",
-                 "point_queries", "candidate_checks", "particle_evals", "staging_nodes", "point_nodes")
+        if uses_warp_kernel(p):
+            names = ("segment_particles", "segment_nodes", "steps", "stagings", "staging_overflows",
+                     "direct_bin_sums", "candidates_staged", "bins", "traversal_iterations",
+                     "particles_tested")
+        else:
+            names = ("segment_particles", "segment_nodes", "steps", "stagings", "staging_overflows",
+                     "point_queries", "candidate_checks", "particle_evals", "staging_nodes", "point_nodes")
         return {k: int(v) for k, v in zip(names, c)}
+
+    def set_kernel_timing(self, enable: bool = True):
+        """Record CUDA events around the kernels of every render (include/aarbf.h)."""
+        self._check(self._lib.aarbf_set_kernel_timing(self._h, int(bool(enable))))
+
+    def kernel_times(self):
+        """(tracking-kernel ms, accumulation-pass ms, renders) summed since the last call."""
+        r, a, k = ctypes.c_double(), ctypes.c_double(), ctypes.c_uint32()
+        self._check(self._lib.aarbf_get_kernel_times(self._h, ctypes.byref(r), ctypes.byref(a),
+                                                     ctypes.byref(k)))
+        return r.value, a.value, k.value
 
     def render_splat(self, params: RenderParams, width: int, height: int, image=None, stream=None):
         p = params.to_c() if isinstance(params, RenderParams) else params

@@ -129,6 +129,22 @@ def orbit_camera(center=(0.5, 0.5, 0.5), distance: float = 2.5, azimuth_deg: flo
             float(2.0 * math.tan(math.radians(fov_deg) / 2.0)))
 
 
+def halton(index: int, base: int) -> float:
+    """Radical inverse of index in base (the Halton sequence, index >= 1)."""
+    f, r = 1.0, 0.0
+    while index > 0:
+        f /= base
+        r += f * (index % base)
+        index //= base
+    return r
+
+
+def halton_jitter(frame: int):
+    """Subpixel jitter of frame k of a TAA sequence: Halton(2, 3) point k + 1, centred on the
+    pixel (offsets in [-0.5, 0.5) pixels)."""
+    return halton(frame + 1, 2) - 0.5, halton(frame + 1, 3) - 0.5
+
+
 def native_params(cam, width: int, height: int, rbf_radius: float, unit: float, density_scale: float,
                   dom, spp: int = 1, frame_id: int = 0, traversal: int = 0, marching: bool = False,
                   majorant: bool = False, bin_length: float = None):

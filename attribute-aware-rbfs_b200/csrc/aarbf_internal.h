@@ -3,8 +3,10 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "../../include/aarbf.h"
 #include "aarbf_device.cuh"
@@ -106,7 +108,9 @@ cudaError_t launch_refit(const float4* rec0, const float* rgeom, uint64_t n, uin
                          uint32_t nleaves, Node* nodes, Node* nodes_ref, const uint32_t* leaf_parent,
                          uint32_t* counters, float* leaf_box, float* leaf_eff, float* root_box,
                          cudaStream_t st);
-cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st);
+// marks (optional): three events recorded before the tracking kernel, between it and the
+// accumulation pass, and after the accumulation pass.
+cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st, const cudaEvent_t* marks = nullptr);
 bool render_uses_warp_kernel(const RenderLaunch& L);
 cudaError_t render_warp_stack_words(size_t* words);
 cudaError_t launch_splat(const RenderLaunch& L, cudaStream_t st);
@@ -149,4 +153,7 @@ struct aarbf_ctx {
   // status word, persistent-kernel work counter, per-sample colour planes
   aarbf::DevBuf status, work, samples, noise_buf, warp_stacks;
   float max_radius = 0.0f;
+  // kernel timing: event triples of timed renders not yet read, and recycled ones
+  bool kernel_timing = false;
+  std::vector<std::array<cudaEvent_t, 3>> ev_pending, ev_free;
 };

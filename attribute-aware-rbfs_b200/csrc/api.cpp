@@ -316,6 +316,9 @@ aarbf_status aarbf_destroy(aarbf_ctx* ctx) {
                     &ctx->fb_accum, &ctx->fb_image, &ctx->status, &ctx->work, &ctx->samples,
                     &ctx->noise_buf, &ctx->warp_stacks};
   for (DevBuf* b : bufs) b->release();
+  for (auto* v : {&ctx->ev_pending, &ctx->ev_free})
+    for (auto& ev : *v)
+      for (cudaEvent_t e : ev) cudaEventDestroy(e);
   delete ctx;
   return AARBF_OK;
 }
@@ -607,7 +610,50 @@ aarbf_status aarbf_render(aarbf_ctx* ctx, const aarbf_params* p, int w, int h, f
     L.noise_w = ctx->noise_w;
     L.noise_h = ctx->noise_h;
   }
-  CK(launch_render(L, (cudaStream_t)stream), "render launch");
+  if (!ctx->kernel_timing) {
+    CK(launch_render(L, (cudaStream_t)stream), "render launch");
+    return AARBF_OK;
+  }
+  std::array<cudaEvent_t, 3> ev{};
+  if (!ctx->ev_free.empty()) {
+    ev = ctx->ev_free.back();
+    ctx->ev_free.pop_back();
+  } else {
+    for (auto& e : ev) CK(cudaEventCreate(&e), "timing event");
+  }
+  ctx->ev_pending.push_back(ev);
+  CK(launch_render(L, (cudaStream_t)stream, ev.data()), "render launch");
+  return AARBF_OK;
+}
+
+aarbf_status aarbf_set_kernel_timing(aarbf_ctx* ctx, int enable) {
+  if (!ctx) return AARBF_ERR_INVALID_ARGUMENT;
+  ctx->kernel_timing = enable != 0;
+  return AARBF_OK;
+}
+
+aarbf_status aarbf_get_kernel_times(aarbf_ctx* ctx, double* render_ms, double* accumulate_ms,
+                                    uint32_t* renders) {
+  if (!ctx) return AARBF_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  double r = 0.0, a = 0.0;
+  uint32_t k = 0;
+  cudaError_t err = cudaSuccess;
+  for (auto& ev : ctx->ev_pending) {
+    float t01 = 0.0f, t12 = 0.0f;
+    if (err == cudaSuccess) err = cudaEventSynchronize(ev[2]);
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&t01, ev[0], ev[1]);
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&t12, ev[1], ev[2]);
+    r += t01;
+    a += t12;
+    ++k;
+    ctx->ev_free.push_back(ev);
+  }
+  ctx->ev_pending.clear();
+  if (err != cudaSuccess) return cuda_fail(ctx, err, "kernel times");
+  if (render_ms) *render_ms = r;
+  if (accumulate_ms) *accumulate_ms = a;
+  if (renders) *renders = k;
   return AARBF_OK;
 }
 

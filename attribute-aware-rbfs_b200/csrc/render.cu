@@ -777,7 +777,8 @@ __device__ float4 raygen_sample(const RenderLaunch& L, uint32_t frame, int px, i
 // ============================================================================================
 
 constexpr int kWarpsPerBlock = 4;
-constexpr int kWarpStack = 8192;      // traversal stack entries per warp (global memory)
+constexpr int kWarpStack = 8192;      // traversal stack entries per warp (global memory: a shared-memory
+                                      // stack costs L1 capacity and measured slower)
 constexpr int kMaxSegBins = 64;       // bins per staged segment
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -1087,47 +1088,55 @@ struct WarpStager {
     }
     return kseg + nbins;
   }
-
-  // direct (unbuffered) majorant sum of one bin
-  __device__ __noinline__ long long bin_sum_direct(const SceneView& s, const Ray& ray, float lo, float hi,
-                                                 uint32_t* status) {
-    long long acc = 0;
-    const float eps = s.eps;
-    warp_traverse(
-        s, stk, buf->leaves, status,
-        [&](float lx, float ly, float lz, float hx, float hy, float hz) {
-          return seg_box(lx, ly, lz, hx, hy, hz, ray.o, inv, lo, hi, eps);
-        },
-        [&](bool v, uint32_t i) -> bool {
-          if (v) acc += fix40(bin_contrib(s, ray, i, lo, hi));
-          return true;
-        },
-        ctr);
-    wctr(ctr, kWcDirect, 1);
-    return warp_sum(acc);
-  }
-
-  // direct point query
-  __device__ __noinline__ void point(const SceneView& s, float3 x, Sample& acc, uint32_t* status) {
-    sample_clear(acc);
-    warp_traverse(
-        s, stk, buf->leaves, status,
-        [&](float lx, float ly, float lz, float hx, float hy, float hz) { return inside(lx, ly, lz, hx, hy, hz, x); },
-        [&](bool v, uint32_t i) -> bool {
-          if (v) eval_particle(s, i, x, acc);
-          return true;
-        },
-        ctr);
-    wctr(ctr, kWcDirect, 1);
-    warp_sum_sample(acc);
-  }
 };
+
+// direct (unbuffered) majorant sum of one bin; out of line (rare path, instruction-cache footprint)
+template <int CAPW>
+__device__ __noinline__ long long warp_bin_sum_direct(const SceneView& s, const Ray ray, const float3 inv, float lo,
+                                                      float hi, WarpBuf<CAPW>* buf, uint32_t* stk, uint32_t* status,
+                                                      unsigned long long* ctr) {
+  long long acc = 0;
+  const float eps = s.eps;
+  warp_traverse(
+      s, stk, buf->leaves, status,
+      [&](float lx, float ly, float lz, float hx, float hy, float hz) {
+        return seg_box(lx, ly, lz, hx, hy, hz, ray.o, inv, lo, hi, eps);
+      },
+      [&](bool v, uint32_t i) -> bool {
+        if (v) acc += fix40(bin_contrib(s, ray, i, lo, hi));
+        return true;
+      },
+      ctr);
+  wctr(ctr, kWcDirect, 1);
+  return warp_sum(acc);
+}
+
+// direct point query; out of line (rare path)
+template <int CAPW>
+__device__ __noinline__ Sample warp_point(const SceneView& s, const float3 x, WarpBuf<CAPW>* buf, uint32_t* stk,
+                                          uint32_t* status, unsigned long long* ctr) {
+  Sample acc;
+  sample_clear(acc);
+  warp_traverse(
+      s, stk, buf->leaves, status,
+      [&](float lx, float ly, float lz, float hx, float hy, float hz) { return inside(lx, ly, lz, hx, hy, hz, x); },
+      [&](bool v, uint32_t i) -> bool {
+        if (v) eval_particle(s, i, x, acc);
+        return true;
+      },
+      ctr);
+  wctr(ctr, kWcDirect, 1);
+  warp_sum_sample(acc);
+  return acc;
+}
 
 // track_majorant with the warp-cooperative stager; same decisions, same random-number stream
 // out of line: one copy serves the primary and the shadow ray (instruction-cache footprint)
+// (the tracker state and the ray are copied into registers for the body: the caller's copies
+// live in local memory because their addresses cross the call)
 template <int CAPW>
-__device__ __noinline__ void track_majorant_warp(const RenderLaunch& L, Tracker& tr, const Ray& ray, WarpBuf<CAPW>* buf,
-                                    uint32_t* stk) {
+__device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, Tracker& tr, const Ray& ray,
+                                                         WarpBuf<CAPW>* buf, uint32_t* stk) {
   WarpStager<CAPW> st;
   st.buf = buf;
   st.stk = stk;
@@ -1194,7 +1203,8 @@ __device__ __noinline__ void track_majorant_warp(const RenderLaunch& L, Tracker&
     int pend_depth[kSplitDepth];
     for (;;) {
       wctr(L.counters, kWcBins, 1);
-      long long acc = direct ? st.bin_sum_direct(L.s, ray, lo, hi, L.status) : st.bin_sum(L.s, ray, k, lo, hi);
+      long long acc = direct ? warp_bin_sum_direct<CAPW>(L.s, ray, st.inv, lo, hi, buf, stk, L.status, L.counters)
+                             : st.bin_sum(L.s, ray, k, lo, hi);
       float M = ((float)acc * kFixInv) * minf;
       if (M > 0.0f) {
         float mid = lo + 0.5f * (hi - lo);
@@ -1220,7 +1230,7 @@ __device__ __noinline__ void track_majorant_warp(const RenderLaunch& L, Tracker&
           if (t >= hi || t >= ray.tmax) break;
           float3 x = make_float3(ray.o.x + t * ray.d.x, ray.o.y + t * ray.d.y, ray.o.z + t * ray.d.z);
           Sample smp;
-          if (direct) st.point(L.s, x, smp, L.status);
+          if (direct) smp = warp_point<CAPW>(L.s, x, buf, stk, L.status, L.counters);
           else st.sample(L.s, k, t, x, smp);
           float D = (float)smp.a0 * kFixInv;
           float sigma = D * scale;
@@ -1244,9 +1254,18 @@ __device__ __noinline__ void track_majorant_warp(const RenderLaunch& L, Tracker&
   tr.t = t;
 }
 
+template <int CAPW>
+__device__ __noinline__ void track_majorant_warp(const RenderLaunch& L, Tracker& tr_io, const Ray& ray_io,
+                                                 WarpBuf<CAPW>* buf, uint32_t* stk) {
+  Tracker tr = tr_io;
+  const Ray ray = ray_io;
+  track_majorant_warp_body<CAPW>(L, tr, ray, buf, stk);
+  tr_io = tr;
+}
+
 // persistent warps; an item is one sample of one pixel, ordered as in k_render
 template <int CAPW>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_render_warp(const RenderLaunch L) {
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_render_warp(const __grid_constant__ RenderLaunch L) {
   extern __shared__ __align__(16) char smem[];
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
   WarpBuf<CAPW>* buf = reinterpret_cast<WarpBuf<CAPW>*>(smem) + wib;
@@ -1285,7 +1304,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_render_warp(const Re
 // different threads at the same time. Each sample's colour goes to its own plane of L.samples;
 // k_accumulate then forms the running mean in sample order (bit-identical to spp launches).
 template <int CAP>
-__global__ void __launch_bounds__(kBlock) k_render(const RenderLaunch L) {
+__global__ void __launch_bounds__(kBlock) k_render(const __grid_constant__ RenderLaunch L) {
   extern __shared__ __align__(16) char smem[];
   const uint32_t tiles_x = (uint32_t)(L.width + 7) / 8u;
   const uint32_t spp = L.spp ? L.spp : 1u;
@@ -1346,7 +1365,7 @@ __global__ void k_accumulate(const RenderLaunch L) {
 }
 
 template <int CAP>
-cudaError_t launch_cap(const RenderLaunch& L, cudaStream_t st) {
+cudaError_t launch_cap(const RenderLaunch& L, cudaStream_t st, const cudaEvent_t* marks) {
   const size_t smem = (sizeof(uint32_t) + 2 * sizeof(float)) * CAP * kBlock;
   static int blocks = 0;
   if (!blocks) {
@@ -1364,11 +1383,14 @@ cudaError_t launch_cap(const RenderLaunch& L, cudaStream_t st) {
   uint64_t items = (uint64_t)((L.width + 7) / 8) * (uint64_t)((L.height + 3) / 4) * 32u * (L.spp ? L.spp : 1u);
   int grid = (int)((items + kBlock - 1) / kBlock);
   if (grid > blocks) grid = blocks;
+  if (marks) cudaEventRecord(marks[0], st);
   k_render<CAP><<<grid, kBlock, smem, st>>>(L);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  if (marks) cudaEventRecord(marks[1], st);
   size_t plane = (size_t)L.width * (size_t)L.height;
   k_accumulate<<<(unsigned)((plane + 255) / 256), 256, 0, st>>>(L);
+  if (marks) cudaEventRecord(marks[2], st);
   return cudaGetLastError();
 }
 
@@ -1396,17 +1418,20 @@ cudaError_t warp_grid(int* blocks) {
 }
 
 template <int CAPW>
-cudaError_t launch_warp(const RenderLaunch& L, cudaStream_t st) {
+cudaError_t launch_warp(const RenderLaunch& L, cudaStream_t st, const cudaEvent_t* marks) {
   int blocks = 0;
   cudaError_t e = warp_grid<CAPW>(&blocks);
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(L.work_counter, 0, sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
+  if (marks) cudaEventRecord(marks[0], st);
   k_render_warp<CAPW><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  if (marks) cudaEventRecord(marks[1], st);
   size_t plane = (size_t)L.width * (size_t)L.height;
   k_accumulate<<<(unsigned)((plane + 255) / 256), 256, 0, st>>>(L);
+  if (marks) cudaEventRecord(marks[2], st);
   return cudaGetLastError();
 }
 
@@ -1427,20 +1452,20 @@ cudaError_t render_warp_stack_words(size_t* words) {
   return e;
 }
 
-cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st) {
+cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st, const cudaEvent_t* marks) {
   if (L.width <= 0 || L.height <= 0) return cudaSuccess;
   if (render_uses_warp_kernel(L)) {
     switch (L.candidate_cap) {
-      case 512: return launch_warp<512>(L, st);
-      case 1024: return launch_warp<1024>(L, st);
-      default: return launch_warp<256>(L, st);
+      case 512: return launch_warp<512>(L, st, marks);
+      case 1024: return launch_warp<1024>(L, st, marks);
+      default: return launch_warp<256>(L, st, marks);
     }
   }
   switch (L.candidate_cap) {
-    case 16: return launch_cap<16>(L, st);
-    case 64: return launch_cap<64>(L, st);
-    case 128: return launch_cap<128>(L, st);
-    default: return launch_cap<32>(L, st);
+    case 16: return launch_cap<16>(L, st, marks);
+    case 64: return launch_cap<64>(L, st, marks);
+    case 128: return launch_cap<128>(L, st, marks);
+    default: return launch_cap<32>(L, st, marks);
   }
 }
 

@@ -245,9 +245,13 @@ __global__ void __launch_bounds__(kBlock) k_splat(const RenderLaunch L, float pa
 
 cudaError_t launch_splat(const RenderLaunch& L, cudaStream_t st) {
   if (L.width <= 0 || L.height <= 0) return cudaSuccess;
-  // a splat sample lies within its particle's radius of the centre, and the centre lies in
-  // its leaf box: padding every box by twice the largest splat radius keeps the test robust
-  float pad = 2.0f * L.splat_rmax + 4.0f * L.s.eps;
+  // An accepted sample point lies within the splat radius of its particle's centre, on the ray
+  // segment being staged. The reference-bounds box holds the sphere of the bounds radius, so
+  // with per-particle splat radii (= bounds radii) the unpadded box already meets the segment;
+  // with the global rbfRadius the sphere can exceed the box by at most rbfRadius. eps covers
+  // the rounding of the sample point and of the box corners.
+  const bool own_radius = (L.flags & kFlagSplatParticleRadius) != 0;
+  float pad = (own_radius ? 0.0f : L.splat_rmax) + 4.0f * L.s.eps;
   dim3 grid((L.width + 15) / 16, (L.height + 7) / 8);
   k_splat<<<grid, kBlock, 0, st>>>(L, pad);
   return cudaGetLastError();

@@ -64,6 +64,11 @@ def parse():
     ap.add_argument("--cap", type=int, default=0,
                     help="staged candidates per ray: 256/512/1024 per warp (majorant), 0 = default")
     ap.add_argument("--plain-spp", type=int, default=1, help="spp of the plain-estimator comparison (0: skip)")
+    ap.add_argument("--marching-spp", type=int, default=1, help="spp of the stochastic-marching variant")
+    ap.add_argument("--taa-frames", type=int, default=64, help="frames of the jittered splat + TAA sequence")
+    ap.add_argument("--no-variants", action="store_true", help="skip the marching / splat / TAA lines")
+    ap.add_argument("--rmse-crop", type=int, default=32, help="side of the centre crop of the RMSE study (0: skip)")
+    ap.add_argument("--rmse-ref-spp", type=int, default=256, help="spp of the FP64 oracle reference of the crop")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
@@ -260,6 +265,104 @@ def config_dict(args):
             "l2": "inputs_larger_than_l2", "parallelism": f"replicas{args.gpus}"}
 
 
+def crop_params(rp, W, H, x0, y0, cw, ch):
+    """Parameters whose cw x ch frame shows pixels [x0, x0+cw) x [y0, y0+ch) of the W x H frame."""
+    import copy
+    q = copy.copy(rp)
+    d00, du, dv = (np.asarray(v, np.float64) for v in (rp.cam_dir00, rp.cam_du, rp.cam_dv))
+    q.cam_dir00 = tuple(float(x) for x in np.float32(d00 + (x0 / W) * du + (y0 / H) * dv))
+    q.cam_du = tuple(float(x) for x in np.float32(du * (cw / W)))
+    q.cam_dv = tuple(float(x) for x in np.float32(dv * (ch / H)))
+    return q
+
+
+def rmse_study(ctx, args, scene, dom, rmax, threads, stream):
+    """RMSE on the centre crop against the FP64 oracle (the same volume model in double precision,
+    an independent random stream, rmse_ref_spp samples): the majorant and the plain GPU estimators
+    at the benchmark's spp."""
+    import torch
+    import oracle.oracle as orc
+    W, H, c = args.width, args.height, args.rmse_crop
+    x0, y0 = W // 2 - c // 2, H // 2 - c // 2
+    p64 = orc.params_from(params_for(args, dom, rmax))
+    t0 = time.perf_counter()
+    ref = scene.render_f64(p64, W, H, (x0, x0 + c, y0, y0 + c), args.rmse_ref_spp, threads=threads)
+    t_ref = time.perf_counter() - t0
+    out = {"crop": [x0, y0, c, c], "spp": args.spp,
+           "reference": f"FP64 oracle, {args.rmse_ref_spp} spp, {threads} threads, {t_ref:.1f} s",
+           "reference_mean": float(ref.mean()), "rmse": {}}
+    for est in ("majorant", "plain"):
+        q = crop_params(params_for(args, dom, rmax, estimator=est, spp=args.spp), W, H, x0, y0, c, c)
+        acc = torch.zeros((c, c, 4), dtype=torch.float32, device="cuda")
+        img = torch.zeros_like(acc)
+        ctx.render(q, c, c, acc, img, stream=stream.cuda_stream)
+        ctx.sync(stream.cuda_stream)
+        g = img[..., :3].cpu().numpy().astype(np.float64)
+        out["rmse"][est + "_gpu"] = float(np.sqrt(((g - ref) ** 2).mean()))
+    return out
+
+
+def variant_timings(ctx, args, dom, rmax, accum, image, stream):
+    """The other estimators of the benchmark configuration's frame, each timed with CUDA events
+    on the launching stream after one warm-up launch (untimed by the headline figure):
+    stochastic marching (blue-noise thresholds), splatting, and a jittered splat + TAA sequence."""
+    import torch
+    from aarbf import scenes
+    W, H = args.width, args.height
+    sp = stream.cuda_stream
+
+    def timed(fn, reps):
+        fn(-1)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for k in range(reps):
+            fn(k)
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    out = {}
+    if args.marching_spp > 0:
+        def march(k):
+            rp = scenes.native_params(scenes.orbit_camera(), W, H, rmax, args.unit, args.density_scale, dom,
+                                      spp=args.marching_spp, frame_id=max(k, 0) * args.marching_spp,
+                                      traversal=args.traversal, marching=True)
+            ctx.render(rp, W, H, accum, image, stream=sp)
+        ms = timed(march, 1)
+        out["marching"] = {"value": W * H * args.marching_spp / ms / 1e3, "unit": UNIT, "ms": ms,
+                           "spp": args.marching_spp,
+                           "estimator": "stochastic marching, step 1 unit, blue-noise thresholds + shadow ray"}
+
+    def splat_params(k):
+        rp = params_for(args, dom, rmax, frame_id=max(k, 0))
+        if k >= 0:
+            rp.jitter_x, rp.jitter_y = scenes.halton_jitter(k)
+        return rp
+
+    ms = timed(lambda k: ctx.render_splat(splat_params(k), W, H, image, stream=sp), 3)
+    out["splat"] = {"value": W * H / ms / 1e3, "unit": "Mpixels/s", "ms_per_frame": ms,
+                    "method": "slabs of 1 unit, 15 nearest particles per slab, over-composited"}
+    if args.taa_frames > 0:
+        prev = torch.zeros_like(image)
+        taa = torch.zeros_like(image)
+        bgra = torch.zeros((H, W), dtype=torch.int32, device=image.device)
+        state = {"prev": prev, "taa": taa}
+
+        def frame(k):
+            ctx.render_splat(splat_params(k), W, H, image, stream=sp)
+            ctx.taa_resolve(image, state["prev"], state["taa"], bgra, W, H, stream=sp)
+            state["prev"], state["taa"] = state["taa"], state["prev"]
+
+        ms = timed(frame, args.taa_frames)
+        ms_taa = timed(lambda k: ctx.taa_resolve(image, state["prev"], state["taa"], bgra, W, H, stream=sp),
+                       args.taa_frames)
+        out["taa_sequence"] = {"frames": args.taa_frames, "ms_per_frame": ms, "value": 1e3 / ms, "unit": "frames/s",
+                               "taa_resolve_ms": ms_taa, "taa_resolve_gbs": 52 * W * H / ms_taa / 1e6,
+                               "jitter": "Halton(2,3)"}
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -309,6 +412,7 @@ def main():
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    ctx.set_kernel_timing(True)
     e0.record(stream)
     for k in range(args.steps):
         step(args.warmup + k)
@@ -316,6 +420,8 @@ def main():
     torch.cuda.synchronize()
     clk = clocks.stop()
     ctx.sync(sp)
+    render_ms, accumulate_ms, timed_renders = ctx.kernel_times()
+    ctx.set_kernel_timing(False)
     t = e0.elapsed_time(e1) / 1e3
     tt = torch.tensor([t], device=dev)
     if world > 1:
@@ -331,7 +437,7 @@ def main():
     counts = ctx.render_count(rp, W, H, accum, image, stream=sp)
     parts, visits = counts["segment_particles"], counts["segment_nodes"]
     alg_bytes = 20 * parts + 64 * visits + 48 * W * H
-    launch_s = t / args.steps
+    launch_s = render_ms / 1e3 / max(timed_renders, 1)
     achieved = alg_bytes / launch_s / 1e9
     peak, peak_kind = measured_peak()
 
@@ -377,13 +483,23 @@ def main():
                "h2d_bytes_per_step": int(sc.xyzw.nbytes + sc.radii.nbytes), "d2h_bytes_per_step": H * W * 16,
                "steps": k_e2e, "ms_per_step": te / k_e2e * 1e3}
 
+    variants = None if args.no_variants else variant_timings(ctx, args, dom, rmax, accum, image, stream)
+
     cpu = None
+    rmse = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         scene = cpu_scene(args, sc, tf, dom, rp.rbf_radius)
         v, r_cpu, dt, desc = cpu_sample(args, scene, rp, args.cpu_seconds, threads)
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc,
                "seconds": round(dt, 2)}
+        if args.rmse_crop > 0 and args.rmse_ref_spp > 0:
+            rmse = rmse_study(ctx, args, scene, dom, rmax, threads, stream)
+            plain_v = plain["value"] if plain else None
+            ms = rmse["rmse"]
+            if plain_v and ms["majorant_gpu"] > 0:
+                rmse["speedup_vs_plain_gpu"] = (value / plain_v) * (ms["plain_gpu"] / ms["majorant_gpu"]) ** 2
+            rmse["speedup_vs_cpu"] = value / v  # the CPU port's images are bit-identical: equal RMSE
 
     if rank == 0:
         line = {
@@ -395,9 +511,11 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profiled_traffic(), "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes, "particles_on_segments": parts,
-                         "node_visits": visits, "kernel_counters": counts},
-            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": args.steps,
-            "build_ms": build_s * 1e3, "plain_estimator": plain,
+                         "node_visits": visits, "kernel": "k_render_warp" if aarbf.uses_warp_kernel(rp)
+                         else "k_render", "kernel_ms": launch_s * 1e3,
+                         "accumulate_ms": accumulate_ms / max(timed_renders, 1), "kernel_counters": counts},
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": 2 * timed_renders,
+            "build_ms": build_s * 1e3, "plain_estimator": plain, "variants": variants, "equal_rmse": rmse,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

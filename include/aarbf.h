@@ -166,10 +166,22 @@ aarbf_status aarbf_render(aarbf_ctx *ctx, const aarbf_params *p, int width, int 
  * (primary [start, termination] and shadow), [1] BVH nodes those segment queries visit, then the
  * kernel's own work: [2] tracking steps, [3] segment stagings, [4] staging overflows, [5] point
  * queries, [6] staged-candidate checks, [7] particle evaluations, [8] node visits while staging,
- * [9] node visits of point queries. Synchronises `stream`. */
+ * [9] node visits of point queries. The ray-per-warp kernel (majorant tracking with
+ * AARBF_TRAVERSAL_AUTO) fills [2..9] with its own work instead: [2] tentative steps, [3] segment
+ * stagings, [4] staging overflows, [5] direct (unstaged) bin sums, [6] candidates staged, [7] bins
+ * and sub-bins visited, [8] warp traversal iterations, [9] particles tested by the traversals.
+ * Synchronises `stream`. */
 #define AARBF_COUNT_SLOTS 10
 aarbf_status aarbf_render_count(aarbf_ctx *ctx, const aarbf_params *p, int width, int height,
                                 float *accum, float *image, uint64_t *counts, void *stream);
+/* Kernel timing (no counterpart in the reference; for roofline figures). While enabled, every
+ * aarbf_render records CUDA events on its stream around its two kernels: the tracking kernel
+ * and the in-order accumulation pass. aarbf_get_kernel_times waits for the recorded events,
+ * returns the summed milliseconds of each kernel and the number of renders timed, and clears
+ * the record. */
+aarbf_status aarbf_set_kernel_timing(aarbf_ctx *ctx, int enable);
+aarbf_status aarbf_get_kernel_times(aarbf_ctx *ctx, double *render_ms, double *accumulate_ms,
+                                    uint32_t *renders);
 /* ParticleSplatRayGen (deviceCodeSplat.hlsl:58-193); writes image only. */
 aarbf_status aarbf_render_splat(aarbf_ctx *ctx, const aarbf_params *p, int width, int height,
                                 float *image, void *stream);

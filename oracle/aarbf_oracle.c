@@ -1370,3 +1370,253 @@ void orc_taa(const float *image, const float *prev, float *taa, uint32_t *bgra, 
     }
   }
 }
+
+/* ------------------------------------------------------------------------------------------ */
+/* FP64 twin: converged reference images of the native-mode volume model                        */
+/* ------------------------------------------------------------------------------------------ */
+/* The same model as the native estimators (extinction sigma = density_scale * D with
+ * D = sum a^3 exp(-4.5 d^2 / r^2) over the particles whose sphere contains the point; colour
+ * pow(C / D, 1 / 2.2); one shadow ray; ambient shading, raygen as deviceCodeRBF.hlsl:206-324),
+ * evaluated in double precision with libm exp/log/pow and an independent 64-bit random stream
+ * (splitmix64). Transfer-function values are interpolated in double from the fp32 tables.
+ * clamp_plain selects the extinction of the plain native estimator, min(sigma, 1/unit).
+ * Delta tracking with per-bin majorants (unbiased for any valid majorant): the expected image
+ * is the model's, whatever the bins. The float BVH only culls: seg_collect inflates every
+ * sphere by 2^-8 r plus an absolute slack far above the float/double ray difference. */
+
+typedef struct {
+  double o[3], d[3], tmax;
+} ray64;
+
+typedef struct {
+  double a, b, tc, h2, r2, w[4];
+  double c[3]; /* centre */
+} cand64;
+
+static uint64_t splitmix64(uint64_t *s) {
+  uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+static double u01(uint64_t *s) { return (double)(splitmix64(s) >> 11) * 0x1p-53; }
+
+static double tex64(const float *tex, int n, int stride, int channel, double u) {
+  /* linear between texel centres, clamp to edge (the parity model of orc_tex_sample) */
+  if (n <= 0) return 0.0;
+  double x = u * (double)n - 0.5;
+  if (!(x > 0.0)) return (double)tex[channel];
+  if (x >= (double)(n - 1)) return (double)tex[(size_t)(n - 1) * stride + channel];
+  int i = (int)floor(x);
+  double f = x - (double)i;
+  double a = (double)tex[(size_t)i * stride + channel], b = (double)tex[(size_t)(i + 1) * stride + channel];
+  return a + (b - a) * f;
+}
+
+static int cmp_cand64(const void *x, const void *y) {
+  double a = ((const cand64 *)x)->a, b = ((const cand64 *)y)->a;
+  return a < b ? -1 : (a > b ? 1 : 0);
+}
+
+typedef struct {
+  cand64 *v;
+  size_t n, cap;
+  orc_cands idx;
+} cand64_set;
+
+static void collect64(const orc_scene *s, const ray64 *r, double t0, double t1, cand64_set *cs) {
+  orc_ray fr;
+  for (int a = 0; a < 3; ++a) {
+    fr.o[a] = (float)r->o[a];
+    fr.d[a] = (float)r->d[a];
+  }
+  fr.tmin = 0.0f;
+  fr.tmax = 1e30f;
+  float m = 1.0f;
+  for (int a = 0; a < 3; ++a) m = fmaxf(m, fabsf(fr.o[a]));
+  seg_collect(s, &fr, (float)t0 - m * 0x1p-12f, (float)t1 + m * 0x1p-12f, &cs->idx);
+  cs->n = 0;
+  for (size_t j = 0; j < cs->idx.n; ++j) {
+    uint64_t i = cs->idx.idx[j];
+    const float *q = s->rec0 + 4 * i;
+    double rr = (double)q[3];
+    if (!(rr > 0.0)) continue;
+    double v[3] = {(double)q[0] - r->o[0], (double)q[1] - r->o[1], (double)q[2] - r->o[2]};
+    double tc = v[0] * r->d[0] + v[1] * r->d[1] + v[2] * r->d[2];
+    double w[3] = {v[0] - tc * r->d[0], v[1] - tc * r->d[1], v[2] - tc * r->d[2]};
+    double h2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+    double r2 = rr * rr;
+    if (!(h2 < r2)) continue;
+    double half = sqrt(r2 - h2);
+    if (tc + half < t0 || tc - half > t1) continue;
+    if (cs->n == cs->cap) {
+      cs->cap = cs->cap ? 2 * cs->cap : 256;
+      cs->v = (cand64 *)realloc(cs->v, cs->cap * sizeof(cand64));
+    }
+    cand64 *c = cs->v + cs->n++;
+    c->a = tc - half;
+    c->b = tc + half;
+    c->tc = tc;
+    c->h2 = h2;
+    c->r2 = r2;
+    for (int a = 0; a < 3; ++a) c->c[a] = (double)q[a];
+    double attr = (double)s->xyzw[4 * i + 3];
+    double al = tex64(s->color, s->nc, 4, 3, attr);
+    double a3 = al * al * al;
+    c->w[0] = a3;
+    for (int k = 0; k < 3; ++k) c->w[1 + k] = pow(tex64(s->color, s->nc, 4, k, attr), 2.2) * a3;
+  }
+  qsort(cs->v, cs->n, sizeof(cand64), cmp_cand64);
+}
+
+/* delta tracking along r from t; returns 1 on a collision (rgb set) */
+static int track64(const orc_scene *s, const orc_params *p, int clamp_plain, const ray64 *r, double t,
+                   uint64_t *rng, cand64_set *cs, size_t **act, size_t *act_cap, double *t_hit,
+                   double *rgb) {
+  const double Lb = (double)p->bin_length > 0.0 ? (double)p->bin_length : 4.0 * (double)p->unit;
+  const double scale = (double)p->density_scale;
+  const double cap = clamp_plain ? 1.0 / (double)p->unit : INFINITY;
+  double chunk = 2.0 * Lb; /* candidates are collected a chunk at a time, chunks growing to 64 bins */
+  while (t < r->tmax) {
+    double c1 = fmin(t + chunk, r->tmax);
+    if (chunk < 64.0 * Lb) chunk *= 2.0;
+    collect64(s, r, t, c1, cs);
+    size_t next = 0, na = 0;
+    if (*act_cap < cs->n + 1) {
+      *act_cap = cs->n + 1;
+      *act = (size_t *)realloc(*act, *act_cap * sizeof(size_t));
+    }
+    size_t *A = *act;
+    for (double lo = t; lo < c1;) {
+      double hi = fmin(lo + Lb, c1);
+      while (next < cs->n && cs->v[next].a <= hi) A[na++] = next++;
+      size_t keep = 0;
+      for (size_t k = 0; k < na; ++k)
+        if (cs->v[A[k]].b >= lo) A[keep++] = A[k];
+      na = keep;
+      if (na == 0) {
+        if (next == cs->n) break; /* nothing further in this chunk */
+        lo = hi;
+        continue;
+      }
+      double M = 0.0;
+      for (size_t k = 0; k < na; ++k) {
+        const cand64 *c = cs->v + A[k];
+        double tcl = fmin(fmax(c->tc, lo), hi), dt = tcl - c->tc;
+        M += c->w[0] * exp(-4.5 * (c->h2 + dt * dt) / c->r2);
+      }
+      M = fmin(M * scale * (1.0 + 1e-9), cap);
+      double tt = lo;
+      while (M > 0.0) {
+        tt += -log(1.0 - u01(rng)) / M;
+        if (tt >= hi) break;
+        double x[3] = {r->o[0] + tt * r->d[0], r->o[1] + tt * r->d[1], r->o[2] + tt * r->d[2]};
+        double acc[4] = {0, 0, 0, 0};
+        for (size_t k = 0; k < na; ++k) {
+          const cand64 *c = cs->v + A[k];
+          double dx = c->c[0] - x[0], dy = c->c[1] - x[1], dz = c->c[2] - x[2];
+          double d2 = dx * dx + dy * dy + dz * dz;
+          if (!(d2 < c->r2)) continue;
+          double rho = exp(-4.5 * d2 / c->r2);
+          for (int q = 0; q < 4; ++q) acc[q] += rho * c->w[q];
+        }
+        double sigma = fmin(acc[0] * scale, cap);
+        if (u01(rng) * M < sigma) {
+          for (int q = 0; q < 3; ++q) rgb[q] = pow(acc[1 + q] / acc[0], 1.0 / 2.2);
+          *t_hit = tt;
+          return 1;
+        }
+      }
+      lo = hi;
+    }
+    t = c1;
+  }
+  return 0;
+}
+
+static void pixel64(const orc_scene *s, const orc_params *p, const double *light, int clamp_plain, int px,
+                    int py, int w, int h, int spp, uint64_t seed, cand64_set *cs, size_t **act,
+                    size_t *act_cap, double *out) {
+  double sum[3] = {0, 0, 0};
+  double lb[3], rt[3];
+  for (int a = 0; a < 3; ++a) {
+    rt[a] = (double)p->aabb_max[a] + 2.0 * (double)p->rbf_radius;
+    lb[a] = (double)p->aabb_min[a] - 2.0 * (double)p->rbf_radius;
+  }
+  uint64_t rng = seed ^ (((uint64_t)(uint32_t)py << 32) | (uint32_t)px) * 0xD1B54A32D192ED03ull;
+  splitmix64(&rng);
+  double sx = ((double)px + 0.5 + (double)p->jitter_x) / (double)w;
+  double sy = ((double)py + 0.5 + (double)p->jitter_y) / (double)h;
+  ray64 r;
+  double n2 = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    r.o[a] = (double)p->cam_pos[a];
+    r.d[a] = (double)p->cam_dir00[a] + sx * (double)p->cam_du[a] + sy * (double)p->cam_dv[a];
+    n2 += r.d[a] * r.d[a];
+  }
+  for (int a = 0; a < 3; ++a) r.d[a] /= sqrt(n2);
+  double te = -INFINITY, tx = INFINITY;
+  for (int a = 0; a < 3; ++a) {
+    double t1 = (lb[a] - r.o[a]) / r.d[a], t2 = (rt[a] - r.o[a]) / r.d[a];
+    te = fmax(te, fmin(t1, t2));
+    tx = fmin(tx, fmax(t1, t2));
+  }
+  te = fmax(te, 0.0);
+  const double amb = (double)p->light_ambient;
+  for (int k = 0; k < spp; ++k) {
+    if (!(te < tx)) break;
+    r.tmax = tx;
+    double rgb[3], th;
+    double t_start = te + (double)p->unit * u01(&rng);
+    if (!track64(s, p, clamp_plain, &r, t_start, &rng, cs, act, act_cap, &th, rgb)) continue;
+    double vis = 1.0;
+    if (amb != 1.0) {
+      ray64 sr;
+      for (int a = 0; a < 3; ++a) {
+        sr.o[a] = r.o[a] + r.d[a] * th;
+        sr.d[a] = light[a];
+      }
+      double ste = -INFINITY, stx = INFINITY;
+      for (int a = 0; a < 3; ++a) {
+        double t1 = (lb[a] - sr.o[a]) / sr.d[a], t2 = (rt[a] - sr.o[a]) / sr.d[a];
+        ste = fmax(ste, fmin(t1, t2));
+        stx = fmin(stx, fmax(t1, t2));
+      }
+      sr.tmax = stx;
+      double srgb[3], sth;
+      if (track64(s, p, clamp_plain, &sr, 0.0, &rng, cs, act, act_cap, &sth, srgb)) vis = 0.0;
+    }
+    for (int q = 0; q < 3; ++q) sum[q] += rgb[q] * vis * (1.0 - amb) + rgb[q] * amb;
+  }
+  for (int q = 0; q < 3; ++q) out[q] = sum[q] / (double)spp;
+}
+
+void orc_render_f64(const orc_scene *s, const orc_params *p, int w, int h, int x0, int x1, int y0, int y1,
+                    int spp, int clamp_plain, uint64_t seed, float *rgb_out, int nthreads) {
+  double az = (double)p->light_azimuth, el = (double)p->light_elevation;
+  double a = el * 3.14 - 0.5 * 3.14, b = (az * 2.0) * 3.14; /* sharedCode.h:127-132 (3.14 as written) */
+  double light[3] = {sin(a) * cos(b), sin(a) * sin(b), cos(a)};
+  int cols = x1 - x0, rows = y1 - y0;
+  long total = (long)rows * (long)cols;
+  int nt = nthreads > 0 ? nthreads : g_threads;
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nt > 0 ? nt : omp_get_max_threads())
+#endif
+  {
+    cand64_set cs = {0, 0, 0, {0, 0, 0}};
+    size_t *act = 0, act_cap = 0;
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 4)
+#endif
+    for (long k = 0; k < total; ++k) {
+      int py = y0 + (int)(k / cols), px = x0 + (int)(k % cols);
+      double out[3];
+      pixel64(s, p, light, clamp_plain, px, py, w, h, spp, seed, &cs, &act, &act_cap, out);
+      for (int q = 0; q < 3; ++q) rgb_out[3 * k + q] = (float)out[q];
+    }
+    free(cs.v);
+    free(cs.idx.idx);
+    free(act);
+  }
+  (void)nt;
+}

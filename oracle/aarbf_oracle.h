@@ -128,6 +128,13 @@ void orc_render_splat(const orc_scene *s, const orc_params *p, int w, int h, flo
 void orc_taa(const float *image, const float *prev, float *taa, uint32_t *bgra, int w, int h,
              int disable);
 
+/* FP64 twin of the native-mode volume model (converged reference images): mean RGB over spp
+ * samples of pixels [x0,x1) x [y0,y1) of a w x h frame, rgb_out 3 floats per pixel, row-major
+ * over the region. clamp_plain: extinction min(density_scale D, 1/unit) of the plain native
+ * estimator instead of density_scale D. Independent random stream (seed). */
+void orc_render_f64(const orc_scene *s, const orc_params *p, int w, int h, int x0, int x1, int y0,
+                    int y1, int spp, int clamp_plain, uint64_t seed, float *rgb_out, int nthreads);
+
 /* per-pixel statistics of the last orc_render call on this thread (steps, queries) */
 void orc_set_threads(int n);
 

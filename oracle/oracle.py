@@ -89,6 +89,8 @@ def lib():
             "orc_render_splat": ([P, ctypes.POINTER(OrcParams), i32, i32, P, i32], None),
             "orc_taa": ([P, P, P, P, i32, i32, i32], None),
             "orc_set_threads": ([i32], None),
+            "orc_render_f64": ([P, ctypes.POINTER(OrcParams), i32, i32, i32, i32, i32, i32, i32, i32, u64, P, i32],
+                               None),
         }
         for k, (a, r) in sigs.items():
             f = getattr(L, k)
@@ -215,6 +217,15 @@ class Scene:
             lib().orc_render_region(self.h, ctypes.byref(params), w, h, x0, x1, y0, y1, _p(accum),
                                     _p(image), threads)
         return accum, image
+
+    def render_f64(self, params, w, h, region, spp, clamp_plain=False, seed=1, threads=0):
+        """FP64 twin of the native volume model: mean RGB over spp samples of the region
+        (x0, x1, y0, y1) of a w x h frame, shape (y1 - y0, x1 - x0, 3)."""
+        x0, x1, y0, y1 = region
+        out = np.zeros((y1 - y0, x1 - x0, 3), np.float32)
+        lib().orc_render_f64(self.h, ctypes.byref(params), w, h, x0, x1, y0, y1, int(spp), int(bool(clamp_plain)),
+                             int(seed), _p(out), threads)
+        return out
 
     def render_splat(self, params, w, h, threads=0):
         image = np.zeros((h, w, 4), np.float32)

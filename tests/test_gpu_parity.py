@@ -249,6 +249,31 @@ def test_render_majorant_tracking(ctx, orc, aarbf_mod, n, ppl, bins, scale, floo
     assert (oi[..., :3] > 0).mean() > 0.01  # the view is not empty
 
 
+def test_kernel_timing(ctx, orc, aarbf_mod):
+    """event timing around the render's kernels leaves the result unchanged and reports one
+    positive duration per kernel for each timed render"""
+    from aarbf import scenes
+    sc = scenes.config_clusters(20_000, clusters=4, seed=9)
+    cm, rm, dm = scenes.tf_linear_ramp()
+    dom = orc.domain([sc.xyzw])
+    w, h = 24, 16
+    rp = scenes.native_params(scenes.orbit_camera(), w, h, float(sc.radii.max()), 0.002, 200.0, dom, spp=2,
+                              majorant=True, bin_length=0.008)
+    scene, *_ = setup_both(ctx, orc, aarbf_mod, sc.xyzw, sc.radii, 4, rp.rbf_radius, tf32=(cm, rm, dm))
+    ctx.set_kernel_timing(True)
+    try:
+        ga, gi = gpu_render(ctx, rp, w, h)
+        ga2, gi2 = gpu_render(ctx, rp, w, h)
+        r_ms, a_ms, k = ctx.kernel_times()
+    finally:
+        ctx.set_kernel_timing(False)
+    assert k == 2 and r_ms > 0 and a_ms > 0
+    assert ctx.kernel_times() == (0.0, 0.0, 0)
+    oa, oi = scene.render(orc.params_from(rp), w, h)
+    assert_radiance(gi, oi, "image")
+    assert_bitexact(gi2, gi, "image (second timed render)")
+
+
 @pytest.mark.parametrize("native", [False, True])
 def test_splat_parity(ctx, orc, aarbf_mod, native):
     w, h = 32, 24

@@ -176,6 +176,31 @@ def test_majorant_estimator_is_unbiased(orc):
     assert abs(means[1] - means[0]) < 0.03 * means[0]
 
 
+@pytest.mark.parametrize("majorant", [True, False])
+def test_fp32_estimators_converge_to_fp64_twin(orc, majorant):
+    """the float estimators (bit-identical to the GPU) agree with the FP64 twin of the volume
+    model up to Monte-Carlo noise: their RMSE against one FP64 image is about that of a second,
+    independent FP64 image of the same spp, and their mean shows no bias"""
+    from aarbf import scenes
+    sc = scenes.config_clusters(50_000, clusters=8, seed=6)
+    tf = scenes.tf_four_peaks()
+    dom = orc.domain([sc.xyzw])
+    w, h, spp = 32, 24, 256
+    rp = scenes.native_params(scenes.orbit_camera(), w, h, float(sc.radii.max()), 0.002, 500.0, dom, spp=spp,
+                              majorant=majorant, bin_length=0.008)
+    scene, _, _ = orc.build_scene(sc.xyzw, sc.radii, dom, 4, rp.rbf_radius, tf, 1 / 255)
+    p = orc.params_from(rp)
+    _, img = scene.render(p, w, h)
+    f32 = img[..., :3].astype(np.float64)
+    ref_a = scene.render_f64(p, w, h, (0, w, 0, h), spp, clamp_plain=not majorant, seed=11).astype(np.float64)
+    ref_b = scene.render_f64(p, w, h, (0, w, 0, h), spp, clamp_plain=not majorant, seed=12).astype(np.float64)
+    assert ref_a.mean() > 0.01  # the view is not empty
+    rmse_f32 = math.sqrt(((f32 - ref_a) ** 2).mean())
+    rmse_f64 = math.sqrt(((ref_b - ref_a) ** 2).mean())
+    assert rmse_f32 < 1.5 * rmse_f64  # heavy-tailed per-pixel noise: a loose factor
+    assert abs(f32.mean() - ref_b.mean()) < 0.03 * ref_b.mean()
+
+
 def test_sort_tie_break(orc):
     """equal Hilbert keys are ordered by (x, y, z, w) then input index"""
     xyzw = np.array([[0.5, 0.5, 0.5, 0.9], [0.5, 0.5, 0.5, 0.1], [0.0, 0.0, 0.0, 0.0], [1, 1, 1, 1],
