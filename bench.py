@@ -88,14 +88,21 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per render launch from the committed ncu summary (scaled there to this
-    workload), or None."""
-    try:
-        with open(os.path.join(ROOT, "profiles", "render_traffic.json")) as f:
-            return json.load(f).get("dram_bytes_per_launch")
-    except Exception:
+def profiled_traffic(args):
+    """DRAM bytes of one render launch of the default workload from the committed ncu summary
+    (profiles/render_traffic.txt), or None for any other workload."""
+    default = (args.particles, args.width, args.height, args.spp, args.estimator) == (
+        10_000_000, 1920, 1080, 16, "majorant")
+    if not default:
         return None
+    try:
+        with open(os.path.join(ROOT, "profiles", "render_traffic.txt")) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return int(line.split(":", 1)[1])
+    except Exception:
+        pass
+    return None
 
 
 class ClockSampler:
@@ -509,7 +516,7 @@ def main():
             "data": "synthetic (seeded generator at the benchmark configuration's sizes and distributions)",
             "config": config_dict(args),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": profiled_traffic(), "peak_kind": peak_kind,
+                         "frac": achieved / peak, "traffic": profiled_traffic(args), "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes, "particles_on_segments": parts,
                          "node_visits": visits, "kernel": "k_render_warp" if aarbf.uses_warp_kernel(rp)
                          else "k_render", "kernel_ms": launch_s * 1e3,
