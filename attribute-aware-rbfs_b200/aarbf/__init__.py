@@ -61,6 +61,7 @@ EXPORTED_SYMBOLS = (
     "aarbf_get_prepass", "aarbf_get_bvh", "aarbf_device_alloc", "aarbf_device_free",
     "aarbf_memcpy", "aarbf_memset", "aarbf_render_count", "aarbf_set_opacity_floor",
     "aarbf_hilbert_sort_noalloc", "aarbf_set_kernel_timing", "aarbf_get_kernel_times",
+    "aarbf_render_diff_forward", "aarbf_render_diff_backward",
 )
 
 
@@ -133,6 +134,8 @@ def _load():
         "aarbf_memset": [P, P, i32, ctypes.c_size_t, P],
         "aarbf_render_count": [P, ctypes.POINTER(Params), i32, i32, P, P, P, P],
         "aarbf_set_kernel_timing": [P, i32],
+        "aarbf_render_diff_forward": [P, ctypes.POINTER(Params), i32, i32, i32, P, P],
+        "aarbf_render_diff_backward": [P, ctypes.POINTER(Params), i32, i32, i32, P, P, P, P, P, P],
         "aarbf_get_kernel_times": [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(u32)],
     }
@@ -395,6 +398,25 @@ class Context:
             names = ("segment_particles", "segment_nodes", "steps", "stagings", "staging_overflows",
                      "point_queries", "candidate_checks", "particle_evals", "staging_nodes", "point_nodes")
         return {k: int(v) for k, v in zip(names, c)}
+
+    @staticmethod
+    def _views(views):
+        vs = [v.to_c() if isinstance(v, RenderParams) else v for v in views]
+        return (Params * len(vs))(*vs), len(vs)
+
+    def render_diff_forward(self, views, width: int, height: int, images, stream=None):
+        """Differentiable form, forward: images (device float32, nviews x height x width x 4)."""
+        arr, nv = self._views(views)
+        self._check(self._lib.aarbf_render_diff_forward(self._h, arr, nv, int(width), int(height), _ptr(images),
+                                                        _stream_ptr(stream)))
+
+    def render_diff_backward(self, views, width: int, height: int, grad_images, grad_xyz, grad_radius, grad_attr,
+                             grad_tf, stream=None):
+        """Adjoint of the last render_diff_forward: gradients in the caller's particle order."""
+        arr, nv = self._views(views)
+        self._check(self._lib.aarbf_render_diff_backward(self._h, arr, nv, int(width), int(height),
+                                                         _ptr(grad_images), _ptr(grad_xyz), _ptr(grad_radius),
+                                                         _ptr(grad_attr), _ptr(grad_tf), _stream_ptr(stream)))
 
     def set_kernel_timing(self, enable: bool = True):
         """Record CUDA events around the kernels of every render (include/aarbf.h)."""

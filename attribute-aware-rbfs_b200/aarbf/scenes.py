@@ -129,6 +129,42 @@ def orbit_camera(center=(0.5, 0.5, 0.5), distance: float = 2.5, azimuth_deg: flo
             float(2.0 * math.tan(math.radians(fov_deg) / 2.0)))
 
 
+@dataclass
+class DiffScene:
+    """Particles of the differentiable form: positions (n, 3), radii (n,), attributes in [0, 1]
+    (n,) and an RGBA transfer function (nc, 4), all float32."""
+    pos: np.ndarray
+    radii: np.ndarray
+    attr: np.ndarray
+    tf: np.ndarray
+
+
+def config_differentiable(n: int = 1_000_000, clusters: int = 16, seed: int = 4, tf_size: int = 64):
+    """(ground truth, initial guess) of the differentiable configuration: a seeded mixture of
+    `clusters` anisotropic Gaussian clusters; ground-truth radii log-uniform in [0.005, 0.02],
+    attribute cluster/clusters + N(0, 0.05); the initial guess has radii 0.01, positions jittered
+    by U(-0.005, 0.005) per axis, attributes perturbed by N(0, 0.05) and a linear-ramp transfer
+    function in place of the ground truth's four peaks."""
+    rng = np.random.default_rng(seed)
+    sc = config_clusters(n, clusters=clusters, background=0.0, seed=seed)
+    r_gt = np.exp(rng.uniform(np.log(0.005), np.log(0.02), n)).astype(np.float32)
+    attr = np.clip(sc.xyzw[:, 3], 0.0, 1.0).astype(np.float32)
+    cm, _, _ = tf_four_peaks(tf_size)
+    gt = DiffScene(np.ascontiguousarray(sc.xyzw[:, :3]), r_gt, attr, cm.astype(np.float32))
+    pos0 = (gt.pos + rng.uniform(-0.005, 0.005, gt.pos.shape)).astype(np.float32)
+    attr0 = np.clip(attr + rng.normal(0.0, 0.05, n), 0.0, 1.0).astype(np.float32)
+    ramp, _, _ = tf_linear_ramp(tf_size)
+    init = DiffScene(pos0, np.full(n, 0.01, np.float32), attr0, ramp.astype(np.float32))
+    return gt, init
+
+
+def orbit_views(count: int = 32, distance: float = 2.5, fov_deg: float = 60.0):
+    """`count` orbit cameras around the unit cube's centre: azimuths evenly spread, elevations
+    alternating between +20 and -20 degrees."""
+    return [orbit_camera(distance=distance, azimuth_deg=360.0 * k / count,
+                         elevation_deg=20.0 if k % 2 == 0 else -20.0, fov_deg=fov_deg) for k in range(count)]
+
+
 def halton(index: int, base: int) -> float:
     """Radical inverse of index in base (the Halton sequence, index >= 1)."""
     f, r = 1.0, 0.0

@@ -114,6 +114,28 @@ cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st, const cudaEven
 bool render_uses_warp_kernel(const RenderLaunch& L);
 cudaError_t render_warp_stack_words(size_t* words);
 cudaError_t launch_splat(const RenderLaunch& L, cudaStream_t st);
+
+// differentiable form (diff.cu)
+struct DiffArgs {
+  SceneView s;
+  const void* views;         // device array: per view 22 words (camera, padded box, unit, gain, frame, spp)
+  int nviews, width, height;
+  float4* image;             // forward output
+  float4* ckpt;              // per-sample checkpoint
+  const float4* grad_image;  // backward input
+  float* g_pos;              // backward accumulators, sorted order
+  float* g_rad;
+  float* g_w;
+  uint32_t* work_counter;
+  uint32_t* status;
+  uint32_t* warp_stacks;
+  bool backward;
+};
+cudaError_t launch_diff(const DiffArgs& A, cudaStream_t st);
+size_t diff_stack_words();
+cudaError_t launch_diff_finish(const float4* xyzw, const uint32_t* perm, uint64_t n, const float4* tf, int nc,
+                               float attr_scale, const float* g_pos, const float* g_rad, const float* g_w,
+                               float* out_pos, float* out_rad, float* out_attr, float* out_tf, cudaStream_t st);
 cudaError_t launch_taa(const float4* image, const float4* prev, float4* taa, uint32_t* bgra, int w,
                        int h, int disable, cudaStream_t st);
 
@@ -153,6 +175,13 @@ struct aarbf_ctx {
   // status word, persistent-kernel work counter, per-sample colour planes
   aarbf::DevBuf status, work, samples, noise_buf, warp_stacks;
   float max_radius = 0.0f;
+  bool radius_map_unit = false;  // every radius-map texel is 1 (required by the differentiable form)
+  // differentiable form: views, per-sample checkpoints, gradient accumulators
+  aarbf::DevBuf diff_views, diff_ckpt, diff_grad;
+  size_t diff_samples = 0;
+  bool diff_ready = false;
+  int diff_nviews = 0, diff_w = 0, diff_h = 0;
+  uint32_t diff_spp = 0;
   // kernel timing: event triples of timed renders not yet read, and recycled ones
   bool kernel_timing = false;
   std::vector<std::array<cudaEvent_t, 3>> ev_pending, ev_free;

@@ -88,6 +88,10 @@ aarbf_status install_tf_f32(aarbf_ctx* ctx, const float* color, int nc, const fl
   ctx->nr = nr;
   ctx->nd = nd;
   ctx->has_tf = true;
+  std::vector<float> rh(nr);
+  CK(cudaMemcpy(rh.data(), ctx->tf_radius.ptr, sizeof(float) * nr, cudaMemcpyDeviceToHost), "tf read");
+  ctx->radius_map_unit = true;
+  for (float v : rh) ctx->radius_map_unit = ctx->radius_map_unit && v == 1.0f;
   return AARBF_OK;
 }
 
@@ -157,12 +161,8 @@ void light_dir(float az, float el, float* dir) {
   dir[2] = std::cos(a);
 }
 
-aarbf_status fill_launch(aarbf_ctx* ctx, const aarbf_params* p, int w, int h, float* accum, float* image,
-                         RenderLaunch& L) {
-  if (!ctx->built) return fail(ctx, AARBF_ERR_NOT_READY, "render before aarbf_build");
-  if (!p || w <= 0 || h <= 0) return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "bad render arguments");
-  memset(&L, 0, sizeof(L));
-  SceneView& s = L.s;
+void fill_scene_view(const aarbf_ctx* ctx, const float* cam_pos, SceneView& s) {
+  memset(&s, 0, sizeof(s));
   s.rec0 = ctx->rec0.as<float4>();
   s.w4 = ctx->w4.as<float4>();
   s.xyzw = ctx->xyzw.as<float4>();
@@ -181,8 +181,16 @@ aarbf_status fill_launch(aarbf_ctx* ctx, const aarbf_params* p, int w, int h, fl
     s.root_lo[a] = ctx->root_box_host[a];
     s.root_hi[a] = ctx->root_box_host[3 + a];
   }
-  s.eps = scene_eps(ctx, p->cam_pos);
+  s.eps = scene_eps(ctx, cam_pos);
   s.per_particle_radius = ctx->has_radii;
+}
+
+aarbf_status fill_launch(aarbf_ctx* ctx, const aarbf_params* p, int w, int h, float* accum, float* image,
+                         RenderLaunch& L) {
+  if (!ctx->built) return fail(ctx, AARBF_ERR_NOT_READY, "render before aarbf_build");
+  if (!p || w <= 0 || h <= 0) return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "bad render arguments");
+  memset(&L, 0, sizeof(L));
+  fill_scene_view(ctx, p->cam_pos, L.s);
   L.accum_id = p->accum_id;
   L.frame_id = p->frame_id;
   L.spp = p->spp ? p->spp : 1;
@@ -314,7 +322,7 @@ aarbf_status aarbf_destroy(aarbf_ctx* ctx) {
                     &ctx->leaf_box, &ctx->root_box,
                     &ctx->sorted_keys, &ctx->tf_color, &ctx->tf_radius, &ctx->tf_density, &ctx->noise,
                     &ctx->fb_accum, &ctx->fb_image, &ctx->status, &ctx->work, &ctx->samples,
-                    &ctx->noise_buf, &ctx->warp_stacks};
+                    &ctx->noise_buf, &ctx->warp_stacks, &ctx->diff_views, &ctx->diff_ckpt, &ctx->diff_grad};
   for (DevBuf* b : bufs) b->release();
   for (auto* v : {&ctx->ev_pending, &ctx->ev_free})
     for (auto& ev : *v)
@@ -682,6 +690,110 @@ aarbf_status aarbf_render_count(aarbf_ctx* ctx, const aarbf_params* p, int w, in
   c.release();
   if (e != cudaSuccess) return cuda_fail(ctx, e, "render count");
   for (int k = 0; k < AARBF_COUNT_SLOTS; ++k) counts[k] = h2[k];
+  return AARBF_OK;
+}
+
+// ---- differentiable form ------------------------------------------------------------------
+
+static aarbf_status diff_setup(aarbf_ctx* ctx, const aarbf_params* views, int nviews, int w, int h, DiffArgs& A,
+                               cudaStream_t st) {
+  if (!ctx->built) return fail(ctx, AARBF_ERR_NOT_READY, "differentiable render before aarbf_build");
+  if (!views || nviews <= 0 || w <= 0 || h <= 0) return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "bad views or size");
+  if (!ctx->radius_map_unit)
+    return fail(ctx, AARBF_ERR_UNSUPPORTED, "differentiable render needs a radius map of ones");
+  if (ctx->nc > 2048) return fail(ctx, AARBF_ERR_UNSUPPORTED, "differentiable render needs <= 2048 colour texels");
+  if (!(ctx->dom[7] > ctx->dom[6])) return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "empty attribute range");
+  const uint32_t spp0 = views[0].spp ? views[0].spp : 1u;
+  std::vector<float> hv(22 * (size_t)nviews);
+  for (int v = 0; v < nviews; ++v) {
+    const aarbf_params* p = views + v;
+    if (!(p->unit > 0.0f)) return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "unit must be > 0");
+    const uint32_t fid = p->frame_id, spp = p->spp ? p->spp : 1u;
+    if (spp != spp0) return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "all views need the same spp");
+    float* o = hv.data() + 22 * (size_t)v;
+    for (int a = 0; a < 3; ++a) {
+      o[a] = p->cam_pos[a];
+      o[3 + a] = p->cam_dir00[a];
+      o[6 + a] = p->cam_du[a];
+      o[9 + a] = p->cam_dv[a];
+      o[12 + a] = p->aabb_min[a] - 2.0f * p->rbf_radius;
+      o[15 + a] = p->aabb_max[a] + 2.0f * p->rbf_radius;
+    }
+    o[18] = p->unit;
+    o[19] = p->density_gain;
+    memcpy(o + 20, &fid, 4);
+    memcpy(o + 21, &spp, 4);
+  }
+  CK(ctx->diff_views.reserve(sizeof(float) * hv.size()), "views alloc");
+  CK(cudaMemcpyAsync(ctx->diff_views.ptr, hv.data(), sizeof(float) * hv.size(), cudaMemcpyHostToDevice, st),
+     "views upload");
+  CK(cudaStreamSynchronize(st), "views upload");
+  memset(&A, 0, sizeof(A));
+  fill_scene_view(ctx, views[0].cam_pos, A.s);
+  for (int v = 1; v < nviews; ++v) A.s.eps = std::fmax(A.s.eps, scene_eps(ctx, views[v].cam_pos));
+  A.views = ctx->diff_views.ptr;
+  A.nviews = nviews;
+  A.width = w;
+  A.height = h;
+  if (!ctx->work.ptr) CK(ctx->work.reserve(256), "work counter");
+  A.work_counter = ctx->work.as<uint32_t>();
+  A.status = ctx->status.as<uint32_t>();
+  CK(ctx->warp_stacks.reserve(4 * diff_stack_words()), "warp stacks");
+  A.warp_stacks = ctx->warp_stacks.as<uint32_t>();
+  ctx->diff_samples = (size_t)nviews * (size_t)w * (size_t)h * spp0;
+  ctx->diff_spp = spp0;
+  return AARBF_OK;
+}
+
+aarbf_status aarbf_render_diff_forward(aarbf_ctx* ctx, const aarbf_params* views, int nviews, int w, int h,
+                                       float* images, void* stream) {
+  if (!ctx || !images) return AARBF_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  DiffArgs A;
+  ctx->diff_ready = false;
+  aarbf_status s = diff_setup(ctx, views, nviews, w, h, A, st);
+  if (s != AARBF_OK) return s;
+  CK(ctx->diff_ckpt.reserve(16 * ctx->diff_samples), "checkpoint alloc");
+  A.image = reinterpret_cast<float4*>(images);
+  A.ckpt = ctx->diff_ckpt.as<float4>();
+  CK(launch_diff(A, st), "diff forward");
+  ctx->diff_ready = true;
+  ctx->diff_nviews = nviews;
+  ctx->diff_w = w;
+  ctx->diff_h = h;
+  return AARBF_OK;
+}
+
+aarbf_status aarbf_render_diff_backward(aarbf_ctx* ctx, const aarbf_params* views, int nviews, int w, int h,
+                                        const float* grad_images, float* grad_xyz, float* grad_radius,
+                                        float* grad_attr, float* grad_tf, void* stream) {
+  if (!ctx || !grad_images || !grad_xyz || !grad_radius || !grad_attr || !grad_tf) return AARBF_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  if (!ctx->diff_ready || ctx->diff_nviews != nviews || ctx->diff_w != w || ctx->diff_h != h || !views ||
+      (views[0].spp ? views[0].spp : 1u) != ctx->diff_spp)
+    return fail(ctx, AARBF_ERR_NOT_READY, "backward without a matching aarbf_render_diff_forward");
+  cudaStream_t st = (cudaStream_t)stream;
+  DiffArgs A;
+  aarbf_status s = diff_setup(ctx, views, nviews, w, h, A, st);
+  if (s != AARBF_OK) return s;
+  const uint64_t n = ctx->n;
+  const size_t nn = n ? n : 1;
+  CK(ctx->diff_grad.reserve(sizeof(float) * 8 * nn), "gradient alloc");
+  float* gp = ctx->diff_grad.as<float>();
+  CK(cudaMemsetAsync(gp, 0, sizeof(float) * 8 * nn, st), "gradient clear");
+  CK(cudaMemsetAsync(grad_tf, 0, sizeof(float) * 4 * (size_t)ctx->nc, st), "gradient clear");
+  A.backward = true;
+  A.ckpt = ctx->diff_ckpt.as<float4>();
+  A.grad_image = reinterpret_cast<const float4*>(grad_images);
+  A.g_pos = gp;
+  A.g_rad = gp + 3 * nn;
+  A.g_w = gp + 4 * nn;
+  CK(launch_diff(A, st), "diff backward");
+  const float scale = 1.0f / (ctx->dom[7] - ctx->dom[6]);  // attribute normalisation
+  CK(launch_diff_finish(ctx->xyzw.as<float4>(), ctx->perm.as<uint32_t>(), n, ctx->tf_color.as<float4>(), ctx->nc,
+                        scale, A.g_pos, A.g_rad, A.g_w, grad_xyz, grad_radius, grad_attr, grad_tf, st),
+     "diff finish");
   return AARBF_OK;
 }
 

@@ -182,6 +182,26 @@ aarbf_status aarbf_render_count(aarbf_ctx *ctx, const aarbf_params *p, int width
 aarbf_status aarbf_set_kernel_timing(aarbf_ctx *ctx, int enable);
 aarbf_status aarbf_get_kernel_times(aarbf_ctx *ctx, double *render_ms, double *accumulate_ms,
                                     uint32_t *renders);
+/* ---- differentiable form (no counterpart in the reference) ------------------------------- */
+
+/* Expected stochastic marching: the reference's stochasticMarching (deviceCodeRBF.hlsl:67-139)
+ * with ambient 1 and its random stopping threshold integrated in closed form, with the
+ * truncated Gaussian shifted to zero at the cut-off radius (continuous in positions and radii).
+ * views: nviews parameter blocks (camera, unit, density_gain, aabb, rbf_radius as the box
+ * padding, frame_id, spp; the same spp in every view; other fields ignored). images: device
+ * float4 nviews x height x width, mean RGB over spp, alpha 1. Keeps a 16-byte checkpoint per
+ * sample for aarbf_render_diff_backward. Needs a built scene whose radius map is all ones and
+ * at most 2048 colour texels. Synchronises `stream` once (view upload). */
+aarbf_status aarbf_render_diff_forward(aarbf_ctx *ctx, const aarbf_params *views, int nviews, int width,
+                                       int height, float *images, void *stream);
+/* Adjoint of the last aarbf_render_diff_forward (same views) by path replay. grad_images:
+ * dL/dimages (device, same layout). Writes, in the caller's particle order: grad_xyz (n x 3),
+ * grad_radius (n), grad_attr (n, the raw attribute: normalisation chained in), and grad_tf
+ * (nc x 4, the RGBA colour table). Accumulation uses float atomics (summation order varies). */
+aarbf_status aarbf_render_diff_backward(aarbf_ctx *ctx, const aarbf_params *views, int nviews, int width,
+                                        int height, const float *grad_images, float *grad_xyz,
+                                        float *grad_radius, float *grad_attr, float *grad_tf, void *stream);
+
 /* ParticleSplatRayGen (deviceCodeSplat.hlsl:58-193); writes image only. */
 aarbf_status aarbf_render_splat(aarbf_ctx *ctx, const aarbf_params *p, int width, int height,
                                 float *image, void *stream);

@@ -1620,3 +1620,340 @@ void orc_render_f64(const orc_scene *s, const orc_params *p, int w, int h, int x
   }
   (void)nt;
 }
+
+/* ------------------------------------------------------------------------------------------ */
+/* Differentiable form: expected stochastic marching, FP64 forward and adjoint                  */
+/* ------------------------------------------------------------------------------------------ */
+/* The reference's stochasticMarching (deviceCodeRBF.hlsl:67-139) stops at the first step where
+ * the accumulated density exceeds -log(1 - 0.99 xi). With ambient = 1 (no shadow ray) the
+ * expectation of its colour over xi has a closed form, which is the differentiable model:
+ *   t_k = t0 + (k + 1) unit,  t0 = tenter + unit u   (u: first LCG draw of the pixel seed)
+ *   D_k = sum rho_i a_i^3,  C_k = sum rho_i a_i^3 rgb_i^2.2  over particles with |x_k - p_i| < r_i,
+ *   rho_i = (exp(-4.5 q^2) - e^-4.5) / (1 - e^-4.5), q = |x_k - p_i| / r_i: the reference's
+ *   truncated Gaussian (evaluate_rbf, sharedCode.h:137-140) shifted to reach 0 at the cut-off, so
+ *   that images are continuous in positions and radii (the unshifted kernel jumps by e^-4.5 at r,
+ *   a change no adjoint sees and finite differences do),
+ *   (rgb_i, a_i) = transfer function at attribute w_i,
+ *   dens_k = min(gain D_k, 1),  tau_k = sum_{j<=k} dens_j,  G_k = min(1, (1 - exp(-tau_k)) / 0.99)
+ *   c_k = (C_k / D_k)^(1/2.2),  E = sum_k (G_k - G_{k-1}) c_k,  pixel = mean of E over spp.
+ * Adjoint (path replay): dE/d dens_j = g'_j c_j + sum_{k>j} B_k with g'_k = dG_k/dtau_k and
+ * B_k = (g'_k - g'_{prev(k)}) c_k, prev(k) the previous step with D > 0; the forward keeps only
+ * B_total = sum_k B_k per sample, the backward replays the ray and subtracts the prefix.
+ * Everything here is double precision: the reference values for the GPU's float kernels and the
+ * subject of the finite-difference checks. Candidates are found by brute force. */
+
+#define DIFF_E45 0.011108996538242306 /* exp(-4.5) */
+#define DIFF_INV (1.0 / (1.0 - DIFF_E45))
+
+typedef struct {
+  int idx;
+  double lo, hi;
+} dcand;
+
+typedef struct {
+  const orc_diff_scene *sc;
+  double *rgb22a3; /* 4 per particle: a^3, rgb^2.2 a^3 */
+} dctx;
+
+static void tf64(const double *tf, int nc, double w, double *out4, int *i0, double *f) {
+  double x = w * (double)nc - 0.5;
+  if (!(x > 0.0)) {
+    *i0 = 0; *f = 0.0;
+  } else if (x >= (double)(nc - 1)) {
+    *i0 = nc - 1; *f = 0.0;
+  } else {
+    *i0 = (int)floor(x); *f = x - (double)*i0;
+  }
+  int j = *i0 + 1 < nc ? *i0 + 1 : *i0;
+  for (int c = 0; c < 4; ++c) out4[c] = tf[4 * *i0 + c] + (tf[4 * j + c] - tf[4 * *i0 + c]) * *f;
+}
+
+typedef struct {
+  double o[3], d[3], t0, tmax;
+  int valid;
+} dray;
+
+static dray diff_ray(const orc_params *p, int px, int py, int w, int h, uint32_t s) {
+  dray r;
+  uint32_t rng = orc_get_rng((int)((p->frame_id + s) & 0xffffu), (uint32_t)px, (uint32_t)py, (uint32_t)w);
+  double u = (double)orc_lcg_next(&rng) * 0x1p-32;
+  double sx = ((double)px + 0.5) / (double)w, sy = ((double)py + 0.5) / (double)h, n2 = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    r.o[a] = (double)p->cam_pos[a];
+    r.d[a] = (double)p->cam_dir00[a] + sx * (double)p->cam_du[a] + sy * (double)p->cam_dv[a];
+    n2 += r.d[a] * r.d[a];
+  }
+  double te = 0.0, tx = 10000.0;
+  for (int a = 0; a < 3; ++a) {
+    r.d[a] /= sqrt(n2);
+    double lb = (double)p->aabb_min[a] - 2.0 * (double)p->rbf_radius;
+    double rt = (double)p->aabb_max[a] + 2.0 * (double)p->rbf_radius;
+    double t1 = (lb - r.o[a]) / r.d[a], t2 = (rt - r.o[a]) / r.d[a];
+    te = fmax(te, fmin(t1, t2));
+    tx = fmin(tx, fmax(t1, t2));
+  }
+  r.valid = te < tx;
+  r.t0 = te + (double)p->unit * u;
+  r.tmax = tx;
+  return r;
+}
+
+/* particles whose sphere meets the ray within [t0, tmax] */
+static int diff_cands(const orc_diff_scene *sc, const dray *r, dcand *out) {
+  int n = 0;
+  for (int i = 0; i < sc->n; ++i) {
+    const double *p = sc->pos + 3 * i;
+    double rr = sc->radius[i];
+    if (!(rr > 0.0)) continue;
+    double v[3] = {p[0] - r->o[0], p[1] - r->o[1], p[2] - r->o[2]};
+    double tc = v[0] * r->d[0] + v[1] * r->d[1] + v[2] * r->d[2];
+    double h2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2] - tc * tc;
+    if (!(h2 < rr * rr)) continue;
+    double half = sqrt(rr * rr - h2);
+    if (tc + half < r->t0 || tc - half > r->tmax) continue;
+    out[n].idx = i;
+    out[n].lo = tc - half;
+    out[n].hi = tc + half;
+    ++n;
+  }
+  return n;
+}
+
+/* one step: D, C and the members (index; kernel value in rho[m], derivative factor in rho[n + m]) */
+static void diff_eval(const dctx *dc, const dray *r, const dcand *cands, int ncand, double t, double *D, double *C,
+                      int *mem, double *rho, int *nm) {
+  const orc_diff_scene *sc = dc->sc;
+  const int n_ = sc->n;
+  double x[3] = {r->o[0] + t * r->d[0], r->o[1] + t * r->d[1], r->o[2] + t * r->d[2]};
+  *D = 0.0;
+  C[0] = C[1] = C[2] = 0.0;
+  *nm = 0;
+  for (int k = 0; k < ncand; ++k) {
+    if (t < cands[k].lo || t > cands[k].hi) continue;
+    int i = cands[k].idx;
+    const double *p = sc->pos + 3 * i;
+    double dx = x[0] - p[0], dy = x[1] - p[1], dz = x[2] - p[2];
+    double d2 = dx * dx + dy * dy + dz * dz, r2 = sc->radius[i] * sc->radius[i];
+    if (!(d2 < r2)) continue;
+    double e = exp(-4.5 * d2 / r2);
+    double q = (e - DIFF_E45) * DIFF_INV;
+    const double *w = dc->rgb22a3 + 4 * i;
+    *D += q * w[0];
+    for (int c = 0; c < 3; ++c) C[c] += q * w[1 + c];
+    if (mem) {
+      mem[*nm] = i;
+      rho[*nm] = q;
+      rho[n_ + *nm] = e * DIFF_INV;
+    }
+    ++*nm;
+  }
+}
+
+/* forward of one sample: colour E and B_total */
+static void diff_sample_fwd(const dctx *dc, const orc_params *p, const dray *r, const dcand *cands, int ncand,
+                            double *E, double *Btot) {
+  double tau = 0.0, G = 0.0, gprev = 0.0;
+  E[0] = E[1] = E[2] = 0.0;
+  Btot[0] = Btot[1] = Btot[2] = 0.0;
+  const double unit = (double)p->unit, gain = (double)p->density_gain;
+  for (int k = 0;; ++k) {
+    double t = r->t0 + (double)(k + 1) * unit;
+    if (t >= r->tmax) break;
+    double D, C[3];
+    int nm;
+    diff_eval(dc, r, cands, ncand, t, &D, C, 0, 0, &nm);
+    if (!(D > 0.0)) continue;
+    double dens = fmin(gain * D, 1.0);
+    tau += dens;
+    double Gk = fmin(1.0, (1.0 - exp(-tau)) / 0.99);
+    double gk = ((1.0 - exp(-tau)) / 0.99 < 1.0) ? exp(-tau) / 0.99 : 0.0;
+    for (int c = 0; c < 3; ++c) {
+      double ck = pow(C[c] / D, 1.0 / 2.2);
+      E[c] += (Gk - G) * ck;
+      Btot[c] += (gk - gprev) * ck;
+    }
+    G = Gk;
+    gprev = gk;
+    if (G >= 1.0) break;
+  }
+}
+
+static void diff_prepare(dctx *dc, const orc_diff_scene *sc) {
+  dc->sc = sc;
+  dc->rgb22a3 = (double *)malloc(sizeof(double) * 4 * (size_t)(sc->n > 0 ? sc->n : 1));
+  for (int i = 0; i < sc->n; ++i) {
+    double t4[4], f;
+    int i0;
+    tf64(sc->tf, sc->nc, sc->attr[i], t4, &i0, &f);
+    double a3 = t4[3] * t4[3] * t4[3];
+    dc->rgb22a3[4 * i] = a3;
+    for (int c = 0; c < 3; ++c) dc->rgb22a3[4 * i + 1 + c] = pow(t4[c], 2.2) * a3;
+  }
+}
+
+double orc_diff_forward(const orc_diff_scene *sc, const orc_params *views, int nviews, int w, int h,
+                        double *images, int nthreads) {
+  dctx dc;
+  diff_prepare(&dc, sc);
+  long total = (long)nviews * w * h;
+  int nt = nthreads > 0 ? nthreads : g_threads;
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nt > 0 ? nt : omp_get_max_threads())
+#endif
+  {
+    dcand *cands = (dcand *)malloc(sizeof(dcand) * (size_t)(sc->n > 0 ? sc->n : 1));
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 8)
+#endif
+    for (long k = 0; k < total; ++k) {
+      int v = (int)(k / ((long)w * h)), pix = (int)(k % ((long)w * h));
+      int px = pix % w, py = pix / w;
+      const orc_params *p = views + v;
+      uint32_t spp = p->spp ? p->spp : 1u;
+      double acc[3] = {0, 0, 0};
+      for (uint32_t s = 0; s < spp; ++s) {
+        dray r = diff_ray(p, px, py, w, h, s);
+        if (!r.valid) continue;
+        int ncand = diff_cands(sc, &r, cands);
+        double E[3], B[3];
+        diff_sample_fwd(&dc, p, &r, cands, ncand, E, B);
+        for (int c = 0; c < 3; ++c) acc[c] += E[c];
+      }
+      for (int c = 0; c < 3; ++c) images[3 * k + c] = acc[c] / (double)spp;
+    }
+    free(cands);
+  }
+  free(dc.rgb22a3);
+  (void)nt;
+  return 0.0;
+}
+
+void orc_diff_backward(const orc_diff_scene *sc, const orc_params *views, int nviews, int w, int h,
+                       const double *grad_images, double *g_pos, double *g_radius, double *g_attr, double *g_tf,
+                       int nthreads) {
+  dctx dc;
+  diff_prepare(&dc, sc);
+  const int n = sc->n, nc = sc->nc;
+  /* per-particle upstream: dL/d(a^3 weight) and dL/d(rgb^2.2 a^3 weight), chained to the TF at the end */
+  size_t nacc = 4 * (size_t)n;
+  memset(g_pos, 0, sizeof(double) * 3 * (size_t)n);
+  memset(g_radius, 0, sizeof(double) * (size_t)n);
+  memset(g_attr, 0, sizeof(double) * (size_t)n);
+  memset(g_tf, 0, sizeof(double) * 4 * (size_t)nc);
+  double *g_w = (double *)calloc(nacc > 0 ? nacc : 1, sizeof(double));
+  long total = (long)nviews * w * h;
+  int nt = nthreads > 0 ? nthreads : g_threads;
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nt > 0 ? nt : omp_get_max_threads())
+#endif
+  {
+    dcand *cands = (dcand *)malloc(sizeof(dcand) * (size_t)(n > 0 ? n : 1));
+    int *mem = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    double *rho = (double *)malloc(sizeof(double) * 2 * (size_t)(n > 0 ? n : 1));
+    double *lp = (double *)calloc(3 * (size_t)n + 1, sizeof(double));
+    double *lr = (double *)calloc((size_t)n + 1, sizeof(double));
+    double *lw = (double *)calloc(nacc + 1, sizeof(double));
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 8)
+#endif
+    for (long k = 0; k < total; ++k) {
+      int v = (int)(k / ((long)w * h)), pix = (int)(k % ((long)w * h));
+      int px = pix % w, py = pix / w;
+      const orc_params *p = views + v;
+      uint32_t spp = p->spp ? p->spp : 1u;
+      const double unit = (double)p->unit, gain = (double)p->density_gain;
+      double g[3];
+      for (int c = 0; c < 3; ++c) g[c] = grad_images[3 * k + c] / (double)spp;
+      for (uint32_t s = 0; s < spp; ++s) {
+        dray r = diff_ray(p, px, py, w, h, s);
+        if (!r.valid) continue;
+        int ncand = diff_cands(sc, &r, cands);
+        double E[3], Btot[3];
+        diff_sample_fwd(&dc, p, &r, cands, ncand, E, Btot);
+        double tau = 0.0, G = 0.0, gprev = 0.0, P[3] = {0, 0, 0};
+        for (int st = 0;; ++st) {
+          double t = r.t0 + (double)(st + 1) * unit;
+          if (t >= r.tmax) break;
+          double D, C[3];
+          int nm;
+          diff_eval(&dc, &r, cands, ncand, t, &D, C, mem, rho, &nm);
+          if (!(D > 0.0)) continue;
+          double dens = fmin(gain * D, 1.0);
+          tau += dens;
+          double Gk = fmin(1.0, (1.0 - exp(-tau)) / 0.99);
+          double gk = ((1.0 - exp(-tau)) / 0.99 < 1.0) ? exp(-tau) / 0.99 : 0.0;
+          double ck[3], grho = 0.0, gD, gC[3];
+          for (int c = 0; c < 3; ++c) {
+            ck[c] = pow(C[c] / D, 1.0 / 2.2);
+            P[c] += (gk - gprev) * ck[c];
+            double S = gk * ck[c] + (Btot[c] - P[c]);
+            grho += g[c] * S;
+          }
+          double wk = Gk - G;
+          gD = (gain * D < 1.0) ? grho * gain : 0.0;
+          for (int c = 0; c < 3; ++c) {
+            double gc = g[c] * wk;
+            gD -= gc * ck[c] / (2.2 * D);
+            gC[c] = (C[c] > 0.0) ? gc * ck[c] / (2.2 * C[c]) : 0.0;
+          }
+          double x[3] = {r.o[0] + t * r.d[0], r.o[1] + t * r.d[1], r.o[2] + t * r.d[2]};
+          for (int m = 0; m < nm; ++m) {
+            int i = mem[m];
+            const double *wi = dc.rgb22a3 + 4 * i;
+            double gr = gD * wi[0] + gC[0] * wi[1] + gC[1] * wi[2] + gC[2] * wi[3];
+            const double *pp = sc->pos + 3 * i;
+            double r2 = sc->radius[i] * sc->radius[i], d2 = 0.0;
+            for (int a = 0; a < 3; ++a) {
+              double dx = x[a] - pp[a];
+              d2 += dx * dx;
+              lp[3 * i + a] += gr * rho[n + m] * 9.0 * dx / r2;
+            }
+            lr[i] += gr * rho[n + m] * 9.0 * d2 / (r2 * sc->radius[i]);
+            lw[4 * i] += gD * rho[m];
+            for (int c = 0; c < 3; ++c) lw[4 * i + 1 + c] += gC[c] * rho[m];
+          }
+          G = Gk;
+          gprev = gk;
+          if (G >= 1.0) break;
+        }
+      }
+    }
+#ifdef _OPENMP
+#pragma omp critical
+#endif
+    {
+      for (size_t j = 0; j < 3 * (size_t)n; ++j) g_pos[j] += lp[j];
+      for (int j = 0; j < n; ++j) g_radius[j] += lr[j];
+      for (size_t j = 0; j < nacc; ++j) g_w[j] += lw[j];
+    }
+    free(cands); free(mem); free(rho); free(lp); free(lr); free(lw);
+  }
+  /* chain the weight gradients to the transfer function and the attribute: the D weight is a^3
+   * and the C weights rgb_c^2.2 a^3, so d/da = 3 a^2 (dA3 + sum_c dC_c rgb_c^2.2) and
+   * d/drgb_c = dC_c 2.2 rgb_c^1.2 a^3 */
+  for (int i = 0; i < n; ++i) {
+    double t4[4], f;
+    int i0;
+    tf64(sc->tf, nc, sc->attr[i], t4, &i0, &f);
+    double a = t4[3], a2 = a * a, a3 = a2 * a;
+    double gtf[4];
+    double ga = g_w[4 * i];
+    for (int c = 0; c < 3; ++c) {
+      double dC = g_w[4 * i + 1 + c];
+      ga += dC * pow(t4[c], 2.2);
+      gtf[c] = (t4[c] > 0.0) ? dC * 2.2 * pow(t4[c], 1.2) * a3 : 0.0;
+    }
+    gtf[3] = ga * 3.0 * a2;
+    int j = i0 + 1 < nc ? i0 + 1 : i0;
+    double x = sc->attr[i] * (double)nc - 0.5;
+    int interior = x > 0.0 && x < (double)(nc - 1);
+    for (int c = 0; c < 4; ++c) {
+      g_tf[4 * i0 + c] += gtf[c] * (1.0 - f);
+      if (j != i0) g_tf[4 * j + c] += gtf[c] * f;
+      if (interior) g_attr[i] += gtf[c] * (sc->tf[4 * j + c] - sc->tf[4 * i0 + c]) * (double)nc;
+    }
+  }
+  free(g_w);
+  free(dc.rgb22a3);
+  (void)nt;
+}

@@ -135,6 +135,21 @@ void orc_taa(const float *image, const float *prev, float *taa, uint32_t *bgra, 
 void orc_render_f64(const orc_scene *s, const orc_params *p, int w, int h, int x0, int x1, int y0,
                     int y1, int spp, int clamp_plain, uint64_t seed, float *rgb_out, int nthreads);
 
+/* Differentiable form (expected stochastic marching, ambient 1), double precision, brute-force
+ * candidate search: particles by position (3n), radius, attribute in [0, 1], and an RGBA
+ * transfer function of nc texels. images: nviews x h x w x 3. The backward takes dL/dimage of
+ * the same shape and writes dL/d(position, radius, attribute, transfer function). Each view's
+ * params give camera, unit, density_gain, aabb, rbf_radius (box padding), frame_id and spp. */
+typedef struct orc_diff_scene {
+  const double *pos, *radius, *attr, *tf;
+  int n, nc;
+} orc_diff_scene;
+double orc_diff_forward(const orc_diff_scene *sc, const orc_params *views, int nviews, int w, int h,
+                        double *images, int nthreads);
+void orc_diff_backward(const orc_diff_scene *sc, const orc_params *views, int nviews, int w, int h,
+                       const double *grad_images, double *g_pos, double *g_radius, double *g_attr,
+                       double *g_tf, int nthreads);
+
 /* per-pixel statistics of the last orc_render call on this thread (steps, queries) */
 void orc_set_threads(int n);
 

@@ -89,6 +89,8 @@ def lib():
             "orc_render_splat": ([P, ctypes.POINTER(OrcParams), i32, i32, P, i32], None),
             "orc_taa": ([P, P, P, P, i32, i32, i32], None),
             "orc_set_threads": ([i32], None),
+            "orc_diff_forward": ([P, P, i32, i32, i32, P, i32], ctypes.c_double),
+            "orc_diff_backward": ([P, P, i32, i32, i32, P, P, P, P, P, i32], None),
             "orc_render_f64": ([P, ctypes.POINTER(OrcParams), i32, i32, i32, i32, i32, i32, i32, i32, u64, P, i32],
                                None),
         }
@@ -231,6 +233,37 @@ class Scene:
         image = np.zeros((h, w, 4), np.float32)
         lib().orc_render_splat(self.h, ctypes.byref(params), w, h, _p(image), threads)
         return image
+
+
+class OrcDiffScene(ctypes.Structure):
+    _fields_ = [("pos", ctypes.c_void_p), ("radius", ctypes.c_void_p), ("attr", ctypes.c_void_p),
+                ("tf", ctypes.c_void_p), ("n", ctypes.c_int), ("nc", ctypes.c_int)]
+
+
+def _diff_args(pos, radius, attr, tf, views):
+    arrs = [np.ascontiguousarray(a, np.float64) for a in (pos, radius, attr, tf)]
+    sc = OrcDiffScene(arrs[0].ctypes.data, arrs[1].ctypes.data, arrs[2].ctypes.data, arrs[3].ctypes.data,
+                      len(arrs[1]), len(arrs[3]))
+    vs = (OrcParams * len(views))(*views)
+    return arrs, sc, vs
+
+
+def diff_forward(pos, radius, attr, tf, views, w, h, threads=0):
+    """FP64 differentiable model (expected stochastic marching): images (nviews, h, w, 3)."""
+    arrs, sc, vs = _diff_args(pos, radius, attr, tf, views)
+    out = np.zeros((len(views), h, w, 3), np.float64)
+    lib().orc_diff_forward(ctypes.byref(sc), vs, len(views), w, h, _p(out), threads)
+    return out
+
+
+def diff_backward(pos, radius, attr, tf, views, w, h, grad_images, threads=0):
+    """FP64 adjoint: (dL/dpos (n,3), dL/dradius (n), dL/dattr (n), dL/dtf (nc,4)) for dL/dimages."""
+    arrs, sc, vs = _diff_args(pos, radius, attr, tf, views)
+    n, nc = len(arrs[1]), len(arrs[3])
+    g = np.ascontiguousarray(grad_images, np.float64)
+    gp, gr, ga, gt = np.zeros((n, 3)), np.zeros(n), np.zeros(n), np.zeros((nc, 4))
+    lib().orc_diff_backward(ctypes.byref(sc), vs, len(views), w, h, _p(g), _p(gp), _p(gr), _p(ga), _p(gt), threads)
+    return gp, gr, ga, gt
 
 
 def build_scene(xyzw, radii, dom, ppl, rbf_radius, tf, alpha_floor=0.0):

@@ -211,3 +211,50 @@ def test_sort_tie_break(orc):
     order = [int(i) for i in perm]
     pos = {i: order.index(i) for i in range(5)}
     assert pos[1] < pos[4] < pos[0]
+
+
+def _diff_case(n=400, w=12, h=12, seed=5):
+    from aarbf import scenes
+    rng = np.random.default_rng(seed)
+    gt, init = scenes.config_differentiable(n, clusters=4, seed=seed, tf_size=16)
+    gt.radii[:] = rng.uniform(0.04, 0.08, n).astype(np.float32)
+    init.radii[:] = 0.06
+    dom = np.array([0, 0, 0, 1, 1, 1, 0, 1], np.float32)
+    views = [scenes.native_params(cam, w, h, 0.08, 0.01, 10.0, dom, spp=2, frame_id=7 * k, marching=True)
+             for k, cam in enumerate(scenes.orbit_views(2))]
+    return gt, init, views
+
+
+def test_diff_adjoint_matches_finite_differences(orc):
+    """the FP64 adjoint of the differentiable form against central differences (h = 1e-3) of the
+    FP64 forward on 48 parameters with non-zero gradient: positions, radii, attributes and
+    transfer-function entries"""
+    gt, init, rviews = _diff_case()
+    w = h = 12
+    views = [orc.params_from(v) for v in rviews]
+    P = [init.pos.astype(np.float64), init.radii.astype(np.float64), init.attr.astype(np.float64),
+         init.tf.astype(np.float64)]
+    target = orc.diff_forward(gt.pos, gt.radii, gt.attr, gt.tf, views, w, h)
+
+    def loss(p):
+        return float(((orc.diff_forward(*p, views, w, h) - target) ** 2).sum())
+
+    img = orc.diff_forward(*P, views, w, h)
+    grads = orc.diff_backward(*P, views, w, h, 2.0 * (img - target))
+    rng = np.random.default_rng(2)
+    an, fd = [], []
+    for kind in range(4):
+        nz = np.argwhere(np.abs(grads[kind]) > 1e-6 * np.abs(grads[kind]).max())
+        for j in rng.choice(len(nz), size=min(12, len(nz)), replace=False):
+            idx = tuple(nz[j])
+            pp = [x.copy() for x in P]
+            pm = [x.copy() for x in P]
+            pp[kind][idx] += 1e-3
+            pm[kind][idx] -= 1e-3
+            fd.append((loss(pp) - loss(pm)) / 2e-3)
+            an.append(grads[kind][idx])
+    an, fd = np.array(an), np.array(fd)
+    assert len(an) == 48
+    cos = an @ fd / (np.linalg.norm(an) * np.linalg.norm(fd))
+    assert cos > 0.999
+    assert np.linalg.norm(an - fd) < 0.03 * np.linalg.norm(fd)
