@@ -37,6 +37,9 @@ TRAVERSAL_STAGED = 0
 TRAVERSAL_POINT = 1     # one BVH point query per tracking step
 TRAVERSAL_THREAD = 2    # per-thread staged segments for every estimator
 
+STORAGE_FP32 = 0
+STORAGE_FP16 = 1        # FP16 positions (relative to 256-particle run origins), attributes, weights
+
 
 def uses_warp_kernel(p) -> bool:
     """True when a render with these parameters runs the ray-per-warp kernel."""
@@ -61,7 +64,8 @@ EXPORTED_SYMBOLS = (
     "aarbf_get_prepass", "aarbf_get_bvh", "aarbf_device_alloc", "aarbf_device_free",
     "aarbf_memcpy", "aarbf_memset", "aarbf_render_count", "aarbf_set_opacity_floor",
     "aarbf_hilbert_sort_noalloc", "aarbf_set_kernel_timing", "aarbf_get_kernel_times",
-    "aarbf_render_diff_forward", "aarbf_render_diff_backward",
+    "aarbf_render_diff_forward", "aarbf_render_diff_backward", "aarbf_batch_create", "aarbf_batch_render",
+    "aarbf_batch_destroy", "aarbf_batch_last_error", "aarbf_set_storage",
 )
 
 
@@ -134,6 +138,10 @@ def _load():
         "aarbf_memset": [P, P, i32, ctypes.c_size_t, P],
         "aarbf_render_count": [P, ctypes.POINTER(Params), i32, i32, P, P, P, P],
         "aarbf_set_kernel_timing": [P, i32],
+        "aarbf_set_storage": [P, i32],
+        "aarbf_batch_create": [ctypes.POINTER(P), P, ctypes.POINTER(Params), i32, P, P, P, P],
+        "aarbf_batch_render": [P, i32, P],
+        "aarbf_batch_destroy": [P],
         "aarbf_render_diff_forward": [P, ctypes.POINTER(Params), i32, i32, i32, P, P],
         "aarbf_render_diff_backward": [P, ctypes.POINTER(Params), i32, i32, i32, P, P, P, P, P, P],
         "aarbf_get_kernel_times": [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
@@ -145,6 +153,8 @@ def _load():
         fn.restype = ctypes.c_int
     lib.aarbf_last_error.argtypes = [P]
     lib.aarbf_last_error.restype = ctypes.c_char_p
+    lib.aarbf_batch_last_error.argtypes = [P]
+    lib.aarbf_batch_last_error.restype = ctypes.c_char_p
     lib.aarbf_status_string.argtypes = [ctypes.c_int]
     lib.aarbf_status_string.restype = ctypes.c_char_p
     return lib
@@ -500,6 +510,10 @@ class Context:
                                             _ptr(le), _ptr(rb)))
         return left, right, nb, lb, le, rb
 
+    def set_storage(self, fp16: bool):
+        """FP16 storage form of the scene the next build makes (aarbf_set_storage)."""
+        self._check(self._lib.aarbf_set_storage(self._h, STORAGE_FP16 if fp16 else STORAGE_FP32))
+
     def set_opacity_floor(self, alpha_floor: float):
         self._check(self._lib.aarbf_set_opacity_floor(self._h, float(alpha_floor)))
 
@@ -536,3 +550,44 @@ def save_series(path: str, frames):
     st = L.aarbf_series_save(path.encode(), ptrs, counts, len(arrs))
     if st:
         raise AarbfError(st, path)
+
+
+class Batch:
+    """Several scenes rendered by one persistent launch (aarbf_batch_create / aarbf_batch_render).
+
+    contexts: built Contexts on one device; params: one RenderParams per scene (majorant
+    tracking); sizes: (width, height) per scene; accums / images: per-scene device framebuffers
+    (float32 H x W x 4). render() only enqueues kernels: it can be captured in a CUDA graph."""
+
+    def __init__(self, contexts, params, sizes, accums, images):
+        self._lib = lib()
+        n = len(contexts)
+        P = ctypes.c_void_p
+        hs = (P * n)(*[c._h for c in contexts])
+        ps = (Params * n)(*[p.to_c() if isinstance(p, RenderParams) else p for p in params])
+        ws = (ctypes.c_int * n)(*[int(w) for w, _ in sizes])
+        hh = (ctypes.c_int * n)(*[int(h) for _, h in sizes])
+        ac = (P * n)(*[_ptr(a) for a in accums])
+        im = (P * n)(*[_ptr(a) for a in images])
+        self._keep = (contexts, accums, images)
+        self._h = P()
+        st = self._lib.aarbf_batch_create(ctypes.byref(self._h), hs, ps, n, ws, hh, ac, im)
+        if st != 0:
+            msg = self._lib.aarbf_last_error(contexts[0]._h).decode()
+            raise AarbfError(st, msg)
+
+    def render(self, candidate_cap: int = 0, stream=None):
+        st = self._lib.aarbf_batch_render(self._h, int(candidate_cap), _stream_ptr(stream))
+        if st != 0:
+            raise AarbfError(st, self._lib.aarbf_batch_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.aarbf_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

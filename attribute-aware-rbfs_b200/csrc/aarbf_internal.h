@@ -54,6 +54,11 @@ struct SceneView {
   float root_lo[3], root_hi[3];
   float eps;      // absolute slack used by conservative culling tests
   int per_particle_radius;
+  // FP16 storage form (null in the fp32 form): packed records the tracking kernels read
+  const uint2* posq;     // FP16 offsets x, y, z from the run origin, FP16 a^3
+  const uint2* colq;     // FP16 rgb^2.2 a^3
+  const float4* origin;  // fp32 origin of every run of 256 particles
+  const float* reval;    // fp32 r_eval
 };
 
 struct RenderLaunch {
@@ -115,6 +120,24 @@ bool render_uses_warp_kernel(const RenderLaunch& L);
 cudaError_t render_warp_stack_words(size_t* words);
 cudaError_t launch_splat(const RenderLaunch& L, cudaStream_t st);
 
+// several scenes in one persistent launch of the ray-per-warp kernel (render.cu)
+struct BatchArgs {
+  const RenderLaunch* launches;  // device: one launch block per scene
+  const uint64_t* item_ofs;      // device: nscenes + 1 prefix sums of work items
+  const uint64_t* pix_ofs;       // device: nscenes + 1 prefix sums of pixels
+  int nscenes;
+  uint64_t total_pixels;
+  int candidate_cap;
+  unsigned long long* work_counter;
+  uint32_t* warp_stacks;
+};
+cudaError_t launch_render_batched(const BatchArgs& B, cudaStream_t st);
+
+// FP16 storage form (fp16.cu)
+cudaError_t launch_quantize_positions(float4* xyzw, uint64_t n, uint2* posq, float4* origin, cudaStream_t st);
+cudaError_t launch_quantize_weights(float4* w4, const float4* rec0, uint64_t n, uint2* posq, uint2* colq,
+                                   float* reval, cudaStream_t st);
+
 // differentiable form (diff.cu)
 struct DiffArgs {
   SceneView s;
@@ -175,6 +198,9 @@ struct aarbf_ctx {
   // status word, persistent-kernel work counter, per-sample colour planes
   aarbf::DevBuf status, work, samples, noise_buf, warp_stacks;
   float max_radius = 0.0f;
+  bool storage_fp16 = false;     // FP16 storage form (takes effect at the next build)
+  bool built_fp16 = false;       // the built scene is in the FP16 form
+  aarbf::DevBuf posq, colq, origin, reval;
   bool radius_map_unit = false;  // every radius-map texel is 1 (required by the differentiable form)
   // differentiable form: views, per-sample checkpoints, gradient accumulators
   aarbf::DevBuf diff_views, diff_ckpt, diff_grad;

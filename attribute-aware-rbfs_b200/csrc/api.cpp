@@ -123,6 +123,10 @@ aarbf_status run_refit(aarbf_ctx* ctx, cudaStream_t st) {
                     ctx->tf_color.as<float4>(), ctx->nc, ctx->tf_radius.as<float>(), ctx->nr, ctx->rbf_radius,
                     ctx->alpha_floor, ctx->rec0.as<float4>(), ctx->w4.as<float4>(), ctx->rgeom.as<float>(), st),
      "prepass");
+  if (ctx->built_fp16)
+    CK(launch_quantize_weights(ctx->w4.as<float4>(), ctx->rec0.as<float4>(), n, ctx->posq.as<uint2>(),
+                               ctx->colq.as<uint2>(), ctx->reval.as<float>(), st),
+       "fp16 weights");
   CK(launch_refit(ctx->rec0.as<float4>(), ctx->rgeom.as<float>(), n, ctx->ppl, ctx->nleaves, ctx->nodes.as<Node>(),
                   ctx->nodes_ref.as<Node>(), ctx->leaf_parent.as<uint32_t>(), ctx->counters.as<uint32_t>(),
                   ctx->leaf_box.as<float>(), ctx->leaf_eff.as<float>(), ctx->root_box.as<float>(), st),
@@ -183,6 +187,12 @@ void fill_scene_view(const aarbf_ctx* ctx, const float* cam_pos, SceneView& s) {
   }
   s.eps = scene_eps(ctx, cam_pos);
   s.per_particle_radius = ctx->has_radii;
+  if (ctx->built_fp16) {
+    s.posq = ctx->posq.as<uint2>();
+    s.colq = ctx->colq.as<uint2>();
+    s.origin = ctx->origin.as<float4>();
+    s.reval = ctx->reval.as<float>();
+  }
 }
 
 aarbf_status fill_launch(aarbf_ctx* ctx, const aarbf_params* p, int w, int h, float* accum, float* image,
@@ -322,7 +332,8 @@ aarbf_status aarbf_destroy(aarbf_ctx* ctx) {
                     &ctx->leaf_box, &ctx->root_box,
                     &ctx->sorted_keys, &ctx->tf_color, &ctx->tf_radius, &ctx->tf_density, &ctx->noise,
                     &ctx->fb_accum, &ctx->fb_image, &ctx->status, &ctx->work, &ctx->samples,
-                    &ctx->noise_buf, &ctx->warp_stacks, &ctx->diff_views, &ctx->diff_ckpt, &ctx->diff_grad};
+                    &ctx->noise_buf, &ctx->warp_stacks, &ctx->diff_views, &ctx->diff_ckpt, &ctx->diff_grad,
+                    &ctx->posq, &ctx->colq, &ctx->origin, &ctx->reval};
   for (DevBuf* b : bufs) b->release();
   for (auto* v : {&ctx->ev_pending, &ctx->ev_free})
     for (auto& ev : *v)
@@ -564,11 +575,20 @@ aarbf_status aarbf_build(aarbf_ctx* ctx, float rbf_radius, uint32_t ppl, void* s
     CK(launch_gather_normalize(in, ctx->has_radii ? ctx->in_radii.as<float>() : nullptr, ctx->perm.as<uint32_t>(), n,
                                dom[6], dom[7], ctx->xyzw.as<float4>(), ctx->radii.as<float>(), st),
        "gather");
+    if (ctx->storage_fp16) {
+      CK(ctx->posq.reserve(8 * nn), "alloc");
+      CK(ctx->colq.reserve(8 * nn), "alloc");
+      CK(ctx->reval.reserve(4 * nn), "alloc");
+      CK(ctx->origin.reserve(16 * ((nn + 255) / 256)), "alloc");
+      CK(launch_quantize_positions(ctx->xyzw.as<float4>(), n, ctx->posq.as<uint2>(), ctx->origin.as<float4>(), st),
+         "fp16 positions");
+    }
     CK(launch_karras(ctx->sorted_keys.as<uint64_t>(), n, ppl, ctx->nleaves, ctx->nodes.as<Node>(),
                      ctx->nodes_ref.as<Node>(), ctx->leaf_parent.as<uint32_t>(), st),
        "karras");
   }
   memcpy(ctx->dom, dom, sizeof(dom));
+  ctx->built_fp16 = ctx->storage_fp16 && n > 0;
   aarbf_status s = run_refit(ctx, st);
   if (s != AARBF_OK) return s;
   if (!n)
@@ -692,6 +712,110 @@ aarbf_status aarbf_render_count(aarbf_ctx* ctx, const aarbf_params* p, int w, in
   for (int k = 0; k < AARBF_COUNT_SLOTS; ++k) counts[k] = h2[k];
   return AARBF_OK;
 }
+
+// ---- batched rendering ---------------------------------------------------------------------
+
+struct aarbf_batch {
+  int device = 0;
+  int nscenes = 0;
+  uint64_t total_pixels = 0;
+  DevBuf dev;           // launch blocks, item and pixel prefix sums, work counter
+  uint32_t* warp_stacks = nullptr;
+  std::string last_error;
+};
+
+aarbf_status aarbf_batch_create(aarbf_batch** out, aarbf_ctx* const* ctxs, const aarbf_params* params, int nscenes,
+                                const int* widths, const int* heights, float* const* accums, float* const* images) {
+  if (!out || !ctxs || !params || nscenes <= 0 || !widths || !heights || !accums || !images)
+    return AARBF_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  aarbf_ctx* c0 = ctxs[0];
+  if (!c0) return AARBF_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(c0->device);
+  std::vector<RenderLaunch> Ls((size_t)nscenes);
+  std::vector<uint64_t> items((size_t)nscenes + 1, 0), pix((size_t)nscenes + 1, 0);
+  for (int i = 0; i < nscenes; ++i) {
+    aarbf_ctx* ctx = ctxs[i];
+    if (!ctx || ctx->device != c0->device)
+      return fail(c0, AARBF_ERR_INVALID_ARGUMENT, "batched scenes need contexts on one device");
+    if (!accums[i] || !images[i]) return fail(c0, AARBF_ERR_INVALID_ARGUMENT, "batched scenes need framebuffers");
+    const aarbf_params& p = params[i];
+    if (!(p.flags & kFlagMajorantTracking) || (p.flags & kFlagBlueNoise) || p.traversal != AARBF_TRAVERSAL_AUTO)
+      return fail(c0, AARBF_ERR_UNSUPPORTED, "batched rendering runs majorant tracking with AARBF_TRAVERSAL_AUTO");
+    aarbf_params q = p;
+    q.candidate_cap = 0;
+    aarbf_status s = fill_launch(ctx, &q, widths[i], heights[i], accums[i], images[i], Ls[(size_t)i]);
+    if (s != AARBF_OK) {
+      c0->last_error = ctx->last_error;
+      return s;
+    }
+    const uint64_t tiles = (uint64_t)((widths[i] + 7) / 8) * (uint64_t)((heights[i] + 3) / 4);
+    items[(size_t)i + 1] = items[(size_t)i] + tiles * 32u * Ls[(size_t)i].spp;
+    pix[(size_t)i + 1] = pix[(size_t)i] + (uint64_t)widths[i] * (uint64_t)heights[i];
+  }
+  size_t words = 0;
+  cudaError_t e0 = render_warp_stack_words(&words);
+  if (e0 == cudaSuccess) e0 = c0->warp_stacks.reserve(4 * words);
+  if (e0 != cudaSuccess) return cuda_fail(c0, e0, "warp stacks");
+  aarbf_batch* b = new aarbf_batch();
+  b->device = c0->device;
+  b->nscenes = nscenes;
+  b->total_pixels = pix.back();
+  b->warp_stacks = c0->warp_stacks.as<uint32_t>();
+  const size_t lb = sizeof(RenderLaunch) * (size_t)nscenes, ob = sizeof(uint64_t) * ((size_t)nscenes + 1);
+  const size_t off_items = (lb + 255) / 256 * 256, off_pix = off_items + (ob + 255) / 256 * 256;
+  const size_t off_ctr = off_pix + (ob + 255) / 256 * 256;
+  cudaError_t e = b->dev.reserve(off_ctr + 256);
+  if (e == cudaSuccess) e = cudaMemcpy(b->dev.ptr, Ls.data(), lb, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(static_cast<char*>(b->dev.ptr) + off_items, items.data(), ob, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(static_cast<char*>(b->dev.ptr) + off_pix, pix.data(), ob, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    b->dev.release();
+    delete b;
+    return cuda_fail(c0, e, "batch upload");
+  }
+  *out = b;
+  return AARBF_OK;
+}
+
+aarbf_status aarbf_batch_render(aarbf_batch* b, int candidate_cap, void* stream) {
+  if (!b) return AARBF_ERR_INVALID_ARGUMENT;
+  if (candidate_cap != 0 && candidate_cap != 256 && candidate_cap != 512 && candidate_cap != 1024) {
+    b->last_error = "candidate_cap must be 0, 256, 512 or 1024";
+    return AARBF_ERR_INVALID_ARGUMENT;
+  }
+  cudaSetDevice(b->device);
+  const size_t lb = sizeof(RenderLaunch) * (size_t)b->nscenes, ob = sizeof(uint64_t) * ((size_t)b->nscenes + 1);
+  const size_t off_items = (lb + 255) / 256 * 256, off_pix = off_items + (ob + 255) / 256 * 256;
+  const size_t off_ctr = off_pix + (ob + 255) / 256 * 256;
+  char* base = static_cast<char*>(b->dev.ptr);
+  BatchArgs B;
+  B.launches = reinterpret_cast<const RenderLaunch*>(base);
+  B.item_ofs = reinterpret_cast<const uint64_t*>(base + off_items);
+  B.pix_ofs = reinterpret_cast<const uint64_t*>(base + off_pix);
+  B.nscenes = b->nscenes;
+  B.total_pixels = b->total_pixels;
+  B.candidate_cap = candidate_cap;
+  B.work_counter = reinterpret_cast<unsigned long long*>(base + off_ctr);
+  B.warp_stacks = b->warp_stacks;
+  cudaError_t e = launch_render_batched(B, (cudaStream_t)stream);
+  if (e != cudaSuccess) {
+    b->last_error = std::string("batch render: ") + cudaGetErrorString(e);
+    return AARBF_ERR_CUDA;
+  }
+  return AARBF_OK;
+}
+
+aarbf_status aarbf_batch_destroy(aarbf_batch* b) {
+  if (!b) return AARBF_OK;
+  cudaSetDevice(b->device);
+  b->dev.release();
+  delete b;
+  return AARBF_OK;
+}
+
+const char* aarbf_batch_last_error(const aarbf_batch* b) { return b ? b->last_error.c_str() : ""; }
 
 // ---- differentiable form ------------------------------------------------------------------
 
@@ -967,6 +1091,15 @@ aarbf_status aarbf_get_prepass(aarbf_ctx* ctx, float* rec0, float* w4, float* rg
   if (rec0) CK(cudaMemcpy(rec0, ctx->rec0.ptr, 16 * n, cudaMemcpyDeviceToHost), "rec0");
   if (w4) CK(cudaMemcpy(w4, ctx->w4.ptr, 16 * n, cudaMemcpyDeviceToHost), "w4");
   if (rgeom) CK(cudaMemcpy(rgeom, ctx->rgeom.ptr, 4 * n, cudaMemcpyDeviceToHost), "rgeom");
+  return AARBF_OK;
+}
+
+aarbf_status aarbf_set_storage(aarbf_ctx* ctx, int format) {
+  if (!ctx) return AARBF_ERR_INVALID_ARGUMENT;
+  if (format != AARBF_STORAGE_FP32 && format != AARBF_STORAGE_FP16)
+    return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "unknown storage format");
+  ctx->storage_fp16 = format == AARBF_STORAGE_FP16;
+  ctx->built = false;
   return AARBF_OK;
 }
 

@@ -10,6 +10,8 @@
 //           shared memory; each step then only scans the staged list. A segment whose candidates
 //           overflow the buffer is halved; below a minimum length the steps fall back to POINT.
 //   POINT:  one stack-based BVH point query per step (the reference's shape).
+#include <cuda_fp16.h>
+
 #include "aarbf_internal.h"
 #include "warp_traverse.cuh"
 
@@ -28,6 +30,29 @@ __device__ __forceinline__ void ctr_add(unsigned long long* c, int i, unsigned l
   if (c) atomicAdd(c + i, v);
 }
 
+// Particle records: the fp32 prepass arrays, or the packed FP16 storage form (fp16.cu) when the
+// scene has one; both decode to the same floats.
+__device__ __forceinline__ float hval16(uint32_t b) { return __half2float(__ushort_as_half((unsigned short)b)); }
+
+__device__ __forceinline__ float4 part_rec(const SceneView& s, uint32_t i) {
+  if (!s.posq) return __ldg(s.rec0 + i);
+  const uint2 q = __ldg(s.posq + i);
+  const float4 o = __ldg(s.origin + (i >> 8));
+  return make_float4(o.x + hval16(q.x & 0xffffu), o.y + hval16(q.x >> 16), o.z + hval16(q.y & 0xffffu),
+                     __ldg(s.reval + i));
+}
+
+__device__ __forceinline__ float part_a3(const SceneView& s, uint32_t i) {
+  if (!s.posq) return __ldg(&s.w4[i].x);
+  return hval16(__ldg(&s.posq[i].y) >> 16);
+}
+
+__device__ __forceinline__ float4 part_w(const SceneView& s, uint32_t i) {
+  if (!s.posq) return __ldg(s.w4 + i);
+  const uint2 c = __ldg(s.colq + i);
+  return make_float4(part_a3(s, i), hval16(c.x & 0xffffu), hval16(c.x >> 16), hval16(c.y & 0xffffu));
+}
+
 struct Sample {
   int count;
   long long a0, a1, a2, a3;
@@ -39,13 +64,13 @@ __device__ __forceinline__ void sample_clear(Sample& s) {
 }
 
 __device__ __forceinline__ void eval_particle(const SceneView& s, uint32_t i, float3 x, Sample& acc) {
-  float4 r = __ldg(s.rec0 + i);
+  float4 r = part_rec(s, i);
   float dx = r.x - x.x, dy = r.y - x.y, dz = r.z - x.z;
   float dist = sqrtf((dx * dx + dy * dy) + dz * dz);
   if (!(dist < r.w)) return;
   float q = (dist * 3.0f) / r.w;  // evaluate_rbf, sigma = 3 (sharedCode.h:137-140)
   float rho = dexp(-0.5f * (q * q));
-  float4 w = __ldg(s.w4 + i);
+  float4 w = part_w(s, i);
   acc.count += 1;
   acc.a0 += fix40(rho * w.x);
   acc.a1 += fix40(rho * w.y);
@@ -195,7 +220,7 @@ struct Stager {
         uint64_t e0 = b0 + s.ppl;
         if (e0 > s.n) e0 = s.n;
         for (uint64_t i = b0; i < e0; ++i) {
-          float4 r = __ldg(s.rec0 + i);
+          float4 r = part_rec(s, i);
           if (!(r.w > 0.0f)) continue;
           float vx = r.x - ray.o.x, vy = r.y - ray.o.y, vz = r.z - ray.o.z;
           float tc = (vx * ray.d.x + vy * ray.d.y) + vz * ray.d.z;
@@ -314,7 +339,7 @@ __device__ void count_segment(const RenderLaunch& L, const Ray& ray, float t0, f
       uint64_t b0 = (uint64_t)leaves[k] * s.ppl, e0 = b0 + s.ppl;
       if (e0 > s.n) e0 = s.n;
       for (uint64_t i = b0; i < e0; ++i) {
-        float4 r = __ldg(s.rec0 + i);
+        float4 r = part_rec(s, i);
         if (!(r.w > 0.0f)) continue;
         float vx = r.x - ray.o.x, vy = r.y - ray.o.y, vz = r.z - ray.o.z;
         float tc = (vx * ray.d.x + vy * ray.d.y) + vz * ray.d.z;
@@ -453,7 +478,7 @@ constexpr int kSplitDepth = 10;
 
 // a^3 rho at particle i's closest approach to [b0, b1]; 0 when its sphere misses the segment
 __device__ __forceinline__ float bin_contrib(const SceneView& s, const Ray& ray, uint32_t i, float b0, float b1) {
-  float4 r = __ldg(s.rec0 + i);
+  float4 r = part_rec(s, i);
   float vx = r.x - ray.o.x, vy = r.y - ray.o.y, vz = r.z - ray.o.z;
   float tc = (vx * ray.d.x + vy * ray.d.y) + vz * ray.d.z;
   float wx = vx - tc * ray.d.x, wy = vy - tc * ray.d.y, wz = vz - tc * ray.d.z;
@@ -464,7 +489,7 @@ __device__ __forceinline__ float bin_contrib(const SceneView& s, const Ray& ray,
   float r2 = r.w * r.w;
   if (!(d2 < r2)) return 0.0f;
   float q2 = (9.0f * d2) / r2;
-  return dexp(-0.5f * q2) * __ldg(&s.w4[i].x);
+  return dexp(-0.5f * q2) * part_a3(s, i);
 }
 
 // majorant sum of one bin without a buffer: every particle of every leaf whose inflated box
@@ -840,7 +865,7 @@ struct WarpStager {
           bool keep = false;
           float a = 0.0f, b = 0.0f;
           if (v) {
-            float4 r = __ldg(s.rec0 + i);
+            float4 r = part_rec(s, i);
             if (r.w > 0.0f) {
               float vx = r.x - ray.o.x, vy = r.y - ray.o.y, vz = r.z - ray.o.z;
               float tc = (vx * ray.d.x + vy * ray.d.y) + vz * ray.d.z;
@@ -1149,37 +1174,78 @@ __device__ __noinline__ void track_majorant_warp(const RenderLaunch& L, Tracker&
 }
 
 // persistent warps; an item is one sample of one pixel, ordered as in k_render
+// items of one render: one sample of one pixel, 32 consecutive items = one sample of an 8x4 tile
+__device__ __forceinline__ uint32_t warp_items(const RenderLaunch& L) {
+  const uint32_t tiles_x = (uint32_t)(L.width + 7) / 8u;
+  const uint32_t spp = L.spp ? L.spp : 1u;
+  return tiles_x * ((uint32_t)(L.height + 3) / 4u) * 32u * spp;
+}
+
+// one work item of the ray-per-warp kernel (all lanes of the warp)
+template <int CAPW>
+__device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t item, WarpBuf<CAPW>* buf,
+                                                 uint32_t* stk) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t tiles_x = (uint32_t)(L.width + 7) / 8u;
+  const uint32_t spp = L.spp ? L.spp : 1u;
+  const size_t plane = (size_t)L.width * (size_t)L.height;
+  const bool cost = (L.flags & kFlagCostImage) != 0;
+  uint32_t group = item >> 5, in = item & 31u;
+  uint32_t tile = group / spp, k = group % spp;
+  const int px = (int)((tile % tiles_x) * 8u + (in & 7u));
+  const int py = (int)((tile / tiles_x) * 4u + (in >> 3));
+  if (px >= L.width || py >= L.height) return;
+  const size_t ofs = (size_t)px + (size_t)L.width * (size_t)py;
+  const long long c0 = cost ? clock64() : 0;
+  float noise = 0.0f;
+  float4 c = raygen_generic(L, (L.frame_id + k) & 0xffffu, px, py, noise, lane == 0,
+                            [&](Tracker& tr, const Ray& r, bool) { track_majorant_warp<CAPW>(L, tr, r, buf, stk); });
+  if (cost) c.w = (float)(clock64() - c0);
+  if (lane == 0) {
+    L.samples[(size_t)k * plane + ofs] = c;
+    if (k + 1 == spp) L.noise_buf[ofs] = noise;
+  }
+}
+
 template <int CAPW>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_render_warp(const __grid_constant__ RenderLaunch L) {
   extern __shared__ __align__(16) char smem[];
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
   WarpBuf<CAPW>* buf = reinterpret_cast<WarpBuf<CAPW>*>(smem) + wib;
   uint32_t* stk = L.warp_stacks + ((size_t)blockIdx.x * kWarpsPerBlock + wib) * kWarpStack;
-  const uint32_t tiles_x = (uint32_t)(L.width + 7) / 8u;
-  const uint32_t spp = L.spp ? L.spp : 1u;
-  const uint32_t total = tiles_x * ((uint32_t)(L.height + 3) / 4u) * 32u * spp;
-  const size_t plane = (size_t)L.width * (size_t)L.height;
-  const bool cost = (L.flags & kFlagCostImage) != 0;
+  const uint32_t total = warp_items(L);
   for (;;) {
     uint32_t item = 0;
     if (lane == 0) item = atomicAdd(L.work_counter, 1u);
     item = __shfl_sync(kFull, item, 0);
     if (item >= total) break;
-    uint32_t group = item >> 5, in = item & 31u;
-    uint32_t tile = group / spp, k = group % spp;
-    const int px = (int)((tile % tiles_x) * 8u + (in & 7u));
-    const int py = (int)((tile / tiles_x) * 4u + (in >> 3));
-    if (px >= L.width || py >= L.height) continue;
-    const size_t ofs = (size_t)px + (size_t)L.width * (size_t)py;
-    const long long c0 = cost ? clock64() : 0;
-    float noise = 0.0f;
-    float4 c = raygen_generic(L, (L.frame_id + k) & 0xffffu, px, py, noise, lane == 0,
-                              [&](Tracker& tr, const Ray& r, bool) { track_majorant_warp<CAPW>(L, tr, r, buf, stk); });
-    if (cost) c.w = (float)(clock64() - c0);
-    if (lane == 0) {
-      L.samples[(size_t)k * plane + ofs] = c;
-      if (k + 1 == spp) L.noise_buf[ofs] = noise;
+    render_warp_item<CAPW>(L, item, buf, stk);
+  }
+}
+
+// Several scenes in one persistent launch: Ls[s] is scene s's launch block, items
+// [item_ofs[s], item_ofs[s + 1]) are its work items; warps take items from one counter.
+template <int CAPW>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 8)
+    k_render_warp_batched(const RenderLaunch* __restrict__ Ls, const uint64_t* __restrict__ item_ofs, int nscenes,
+                          unsigned long long* work_counter, uint32_t* warp_stacks) {
+  extern __shared__ __align__(16) char smem[];
+  const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+  WarpBuf<CAPW>* buf = reinterpret_cast<WarpBuf<CAPW>*>(smem) + wib;
+  uint32_t* stk = warp_stacks + ((size_t)blockIdx.x * kWarpsPerBlock + wib) * kWarpStack;
+  const uint64_t total = item_ofs[nscenes];
+  for (;;) {
+    unsigned long long item = 0;
+    if (lane == 0) item = atomicAdd(work_counter, 1ull);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= total) break;
+    int lo = 0, hi = nscenes;  // item_ofs[lo] <= item < item_ofs[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (item_ofs[mid] <= item) lo = mid;
+      else hi = mid;
     }
+    render_warp_item<CAPW>(Ls[lo], (uint32_t)(item - item_ofs[lo]), buf, stk);
   }
 }
 
@@ -1215,10 +1281,9 @@ __global__ void __launch_bounds__(kBlock) k_render(const __grid_constant__ Rende
 }
 
 // running mean over the samples in order, deviceCodeRBF.hlsl:326-335
-__global__ void k_accumulate(const RenderLaunch L) {
+// running mean of one pixel's samples in sample order (deviceCodeRBF.hlsl:326-335)
+__device__ __forceinline__ void accumulate_pixel(const RenderLaunch& L, size_t ofs) {
   const size_t plane = (size_t)L.width * (size_t)L.height;
-  const size_t ofs = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (ofs >= plane) return;
   const uint32_t spp = L.spp ? L.spp : 1u;
   const bool cost = (L.flags & kFlagCostImage) != 0;
   float4 prev = L.accum[ofs];
@@ -1247,6 +1312,27 @@ __global__ void k_accumulate(const RenderLaunch L) {
   // diagnostic: the image's alpha channel receives the pixel's cost in SM clock cycles
   if (cost) fin.w = cycles;
   L.image[ofs] = fin;
+}
+
+__global__ void k_accumulate(const RenderLaunch L) {
+  const size_t plane = (size_t)L.width * (size_t)L.height;
+  const size_t ofs = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (ofs >= plane) return;
+  accumulate_pixel(L, ofs);
+}
+
+// the accumulation pass of every scene of a batch: pixels [pix_ofs[s], pix_ofs[s + 1]) are scene s's
+__global__ void k_accumulate_batched(const RenderLaunch* __restrict__ Ls, const uint64_t* __restrict__ pix_ofs,
+                                     int nscenes) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= pix_ofs[nscenes]) return;
+  int lo = 0, hi = nscenes;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (pix_ofs[mid] <= i) lo = mid;
+    else hi = mid;
+  }
+  accumulate_pixel(Ls[lo], (size_t)(i - pix_ofs[lo]));
 }
 
 template <int CAP>
@@ -1335,6 +1421,40 @@ cudaError_t render_warp_stack_words(size_t* words) {
   int blocks = max(b0, max(b1, b2));
   *words = (size_t)blocks * kWarpsPerBlock * kWarpStack;
   return e;
+}
+
+namespace {
+template <int CAPW>
+cudaError_t launch_warp_batched(const BatchArgs& B, cudaStream_t st) {
+  int blocks = 0;
+  cudaError_t e = warp_grid<CAPW>(&blocks);
+  if (e != cudaSuccess) return e;
+  static bool configured = false;
+  if (!configured) {
+    e = cudaFuncSetAttribute(k_render_warp_batched<CAPW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(WarpBuf<CAPW>) * kWarpsPerBlock));
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  e = cudaMemsetAsync(B.work_counter, 0, sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+  k_render_warp_batched<CAPW><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(
+      B.launches, B.item_ofs, B.nscenes, B.work_counter, B.warp_stacks);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (B.total_pixels)
+    k_accumulate_batched<<<(unsigned)((B.total_pixels + 255) / 256), 256, 0, st>>>(B.launches, B.pix_ofs, B.nscenes);
+  return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_render_batched(const BatchArgs& B, cudaStream_t st) {
+  if (B.nscenes <= 0) return cudaSuccess;
+  switch (B.candidate_cap) {
+    case 512: return launch_warp_batched<512>(B, st);
+    case 1024: return launch_warp_batched<1024>(B, st);
+    default: return launch_warp_batched<256>(B, st);
+  }
 }
 
 cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st, const cudaEvent_t* marks) {

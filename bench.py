@@ -69,6 +69,12 @@ def parse():
     ap.add_argument("--no-variants", action="store_true", help="skip the marching / splat / TAA lines")
     ap.add_argument("--rmse-crop", type=int, default=32, help="side of the centre crop of the RMSE study (0: skip)")
     ap.add_argument("--rmse-ref-spp", type=int, default=256, help="spp of the FP64 oracle reference of the crop")
+    ap.add_argument("--diff-views", type=int, default=32,
+                    help="views of the differentiable-form measurement (1M particles, 512x512, 8 spp; 0: skip)")
+    ap.add_argument("--batch-scenes", type=int, default=64,
+                    help="scenes of the batched-rendering measurement (0: skip)")
+    ap.add_argument("--precision-particles", type=int, default=100_000_000,
+                    help="particles of the fp32/FP16 storage comparison (0: skip)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
@@ -298,15 +304,257 @@ def rmse_study(ctx, args, scene, dom, rmax, threads, stream):
     out = {"crop": [x0, y0, c, c], "spp": args.spp,
            "reference": f"FP64 oracle, {args.rmse_ref_spp} spp, {threads} threads, {t_ref:.1f} s",
            "reference_mean": float(ref.mean()), "rmse": {}}
-    for est in ("majorant", "plain"):
-        q = crop_params(params_for(args, dom, rmax, estimator=est, spp=args.spp), W, H, x0, y0, c, c)
+    imgs = {}
+    for est in ("majorant", "plain", "majorant_fp16"):
+        if est == "majorant_fp16":  # the same scene in the FP16 storage form
+            ctx.set_storage(True)
+            ctx.build(rmax, args.ppl, stream=stream.cuda_stream)
+        q = crop_params(params_for(args, dom, rmax, estimator=est.split("_")[0], spp=args.spp), W, H, x0, y0, c, c)
         acc = torch.zeros((c, c, 4), dtype=torch.float32, device="cuda")
         img = torch.zeros_like(acc)
         ctx.render(q, c, c, acc, img, stream=stream.cuda_stream)
         ctx.sync(stream.cuda_stream)
         g = img[..., :3].cpu().numpy().astype(np.float64)
+        imgs[est] = g
         out["rmse"][est + "_gpu"] = float(np.sqrt(((g - ref) ** 2).mean()))
+    ctx.set_storage(False)
+    ctx.build(rmax, args.ppl, stream=stream.cuda_stream)
+    # storage rounding alone: FP16 against fp32 form with the same random streams
+    out["rmse_fp16_vs_fp32_same_stream"] = float(np.sqrt(((imgs["majorant_fp16"] - imgs["majorant"]) ** 2).mean()))
     return out
+
+
+def precision_timing(args, dev, stream):
+    """The precision configuration: precision_particles particles of the benchmark distribution,
+    1920x1080, 4 spp, majorant tracking, in the fp32 and the FP16 storage form (same random
+    streams); CUDA events on the stream, one untimed render first, then the mean of two. Reports
+    Mrays/s of each form and the RMSE between their images."""
+    import torch
+    import aarbf
+    from aarbf import scenes
+    sc = scenes.config_clusters(args.precision_particles, seed=2)
+    cm, rm, dm = scenes.tf_four_peaks()
+    dom = domain_of(sc.xyzw)
+    rmax = float(sc.radii.max())
+    W, H, S = args.width, args.height, 4
+    ctx = aarbf.Context(dev.index or 0)
+    sp = stream.cuda_stream
+    ctx.set_domain(dom)
+    ctx.set_transfer_functions_f32(cm, rm, dm)
+    ctx.set_opacity_floor(args.alpha_floor)
+    xyzw = torch.from_numpy(sc.xyzw).pin_memory()
+    radii = torch.from_numpy(sc.radii).pin_memory()
+    del sc
+    out = {"particles": args.precision_particles, "width": W, "height": H, "spp": S}
+    imgs = {}
+    for form in ("fp32", "fp16"):
+        ctx.set_storage(form == "fp16")
+        ctx.set_particles(xyzw, radii, stream=sp)
+        ctx.build(rmax, args.ppl, stream=sp)
+        acc = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)
+        img = torch.zeros_like(acc)
+        rp = params_for(args, dom, rmax, spp=S)
+        ctx.render(rp, W, H, acc, img, stream=sp)
+        ctx.sync(sp)
+        ctx.set_kernel_timing(True)
+        for _ in range(2):
+            ctx.render(rp, W, H, acc, img, stream=sp)
+        r_ms, _, k = ctx.kernel_times()
+        ctx.set_kernel_timing(False)
+        ms = r_ms / k
+        out[form] = {"kernel_ms": ms, "mrays_s": W * H * S / ms / 1e3}
+        imgs[form] = img[..., :3].double()
+    out["rmse_fp16_vs_fp32_same_stream"] = float(((imgs["fp16"] - imgs["fp32"]) ** 2).mean().sqrt())
+    out["speedup_fp16"] = out["fp16"]["mrays_s"] / out["fp32"]["mrays_s"]
+    ctx.close()
+    return out
+
+
+def differentiable_timing(args, dev, stream):
+    """The differentiable configuration: 1M particles in 16 clusters, learnable positions, radii,
+    attributes and 64-entry RGBA transfer function, diff_views target views of 512x512 at 8 spp,
+    expected stochastic marching (unit 0.005 = half the initial radius, density scale 50), L2
+    image loss. One iteration = forward of every view + the adjoint; CUDA events on the stream,
+    one untimed iteration first, then the mean of two."""
+    import torch
+    import aarbf
+    from aarbf import scenes
+    W = H = 512
+    n = 1_000_000
+    gt, init = scenes.config_differentiable(n)
+    dom = np.array([0, 0, 0, 1, 1, 1, 0, 1], np.float32)
+    views = [scenes.native_params(cam, W, H, 0.02, 0.005, 50.0, dom, spp=8, frame_id=8 * k, marching=True)
+             for k, cam in enumerate(scenes.orbit_views(32)[:args.diff_views])]
+    nv = len(views)
+    ctx = aarbf.Context(dev.index or 0)
+    sp = stream.cuda_stream
+    ctx.set_domain(dom)
+
+    def setup(sc):
+        nc = len(sc.tf)
+        ctx.set_transfer_functions_f32(sc.tf, np.ones(nc, np.float32), np.ones(nc, np.float32))
+        ctx.set_particles(np.concatenate([sc.pos, sc.attr[:, None]], 1).astype(np.float32), sc.radii, stream=sp)
+        ctx.build(float(sc.radii.max()), 8, stream=sp)
+
+    img = torch.zeros((nv, H, W, 4), dtype=torch.float32, device=dev)
+    setup(gt)
+    ctx.render_diff_forward(views, W, H, img, stream=sp)
+    ctx.sync(sp)
+    target = img.clone()
+    setup(init)
+    g = torch.zeros_like(img)
+    gp = torch.zeros((n, 3), device=dev)
+    gr = torch.zeros(n, device=dev)
+    ga = torch.zeros(n, device=dev)
+    gtf = torch.zeros((64, 4), device=dev)
+    fwd, tot = [], []
+    with torch.cuda.stream(stream):
+        for it in range(3):
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            ctx.render_diff_forward(views, W, H, img, stream=sp)
+            e1.record(stream)
+            torch.sub(img, target, out=g)
+            g.mul_(2.0)
+            g[..., 3] = 0.0
+            ctx.render_diff_backward(views, W, H, g, gp, gr, ga, gtf, stream=sp)
+            e2.record(stream)
+            torch.cuda.synchronize()
+            ctx.sync(sp)
+            if it > 0:
+                fwd.append(e0.elapsed_time(e1))
+                tot.append(e0.elapsed_time(e2))
+    ctx.close()
+    f, t = sum(fwd) / len(fwd), sum(tot) / len(tot)
+    return {"config": f"1M particles, 16 clusters, {nv} views 512x512, 8 spp, expected stochastic marching "
+                      "(unit 0.005, density scale 50), L2 image loss; gradients for positions, radii, attributes "
+                      "and the 64-entry RGBA transfer function",
+            "fwd_ms": f, "fwd_bwd_ms_per_iter": t, "bwd_over_fwd": (t - f) / f, "fwd_bwd_over_fwd": t / f,
+            "rays_per_iter": nv * W * H * 8}
+
+
+def batched_timing(args, dev, stream):
+    """The batched configuration: batch_scenes independent scenes, particle counts log-uniform in
+    [10k, 5M] from seeded Gaussian-cluster mixtures (8-64 clusters) with their own four-peak
+    transfer functions, orbit cameras at random azimuth/elevation, resolutions from
+    {256^2, 512^2, 1024^2}, 1-16 spp, majorant tracking. Timed with CUDA events: every scene
+    rendered by its own launch in sequence, and all scenes in one persistent launch replayed
+    from a CUDA graph with the launch shape the autotuner picked (tuned on a 1-spp copy of the
+    batch). The plain estimator (global majorant, thread per sample) is timed on the first
+    eight scenes at 1 spp."""
+    import torch
+    import aarbf
+    from aarbf import autotune, scenes
+    rng = np.random.default_rng(55)
+    sp = stream.cuda_stream
+    ctxs, params, sizes, accs, imgs = [], [], [], [], []
+    particles = 0
+    for k in range(args.batch_scenes):
+        n = int(np.exp(rng.uniform(np.log(1e4), np.log(5e6))))
+        sc = scenes.config_clusters(n, clusters=int(rng.integers(8, 65)), seed=100 + k)
+        cm, rm, dm = scenes.tf_four_peaks(256, seed=200 + k)
+        dom = domain_of(sc.xyzw)
+        c = aarbf.Context(dev.index or 0)
+        c.set_domain(dom)
+        c.set_transfer_functions_f32(cm, rm, dm)
+        c.set_opacity_floor(1.0 / 255.0)
+        c.set_particles(sc.xyzw, sc.radii, stream=sp)
+        c.build(float(sc.radii.max()), 8, stream=sp)
+        res = int(rng.choice([256, 512, 1024]))
+        spp = int(rng.integers(1, 17))
+        cam = scenes.orbit_camera(azimuth_deg=float(rng.uniform(0, 360)), elevation_deg=float(rng.uniform(-40, 40)))
+        params.append(scenes.native_params(cam, res, res, float(sc.radii.max()), args.unit, args.density_scale, dom,
+                                           spp=spp, frame_id=k * 16, majorant=True, bin_length=args.bin * args.unit))
+        ctxs.append(c)
+        sizes.append((res, res))
+        accs.append(torch.zeros((res, res, 4), dtype=torch.float32, device=dev))
+        imgs.append(torch.zeros((res, res, 4), dtype=torch.float32, device=dev))
+        particles += n
+    rays = sum(w * h * int(p.spp) for p, (w, h) in zip(params, sizes))
+    torch.cuda.synchronize()
+
+    def events():
+        return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    # every scene by its own launch, in sequence
+    for c, p, (w, h), a, i in zip(ctxs, params, sizes, accs, imgs):
+        c.render(p, w, h, a, i, stream=sp)
+    torch.cuda.synchronize()
+    e0, e1 = events()
+    e0.record(stream)
+    for c, p, (w, h), a, i in zip(ctxs, params, sizes, accs, imgs):
+        c.render(p, w, h, a, i, stream=sp)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_seq = e0.elapsed_time(e1)
+    ref = [i.clone() for i in imgs]
+    # autotune on a 1-spp copy, then one launch in a CUDA graph
+    import copy
+    proxy = []
+    for p in params:
+        q = copy.copy(p)
+        q.spp = 1
+        proxy.append(q)
+    cap, bins, table = autotune.tune_batch(ctxs, proxy, sizes, accs, imgs, stream)
+    tuned = []
+    for p in params:
+        q = copy.copy(p)
+        q.stage_bins = bins
+        tuned.append(q)
+    b = aarbf.Batch(ctxs, tuned, sizes, accs, imgs)
+    with torch.cuda.stream(stream):
+        b.render(cap, stream)
+        torch.cuda.synchronize()
+        e0, e1 = events()
+        e0.record(stream)
+        b.render(cap, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_direct = e0.elapsed_time(e1)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        b.render(cap, stream)
+    for i in imgs:
+        i.zero_()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):  # replay on the timed stream
+        g.replay()
+        torch.cuda.synchronize()
+        for i in imgs:
+            i.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = events()
+        e0.record(stream)
+        g.replay()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    t_graph = e0.elapsed_time(e1)
+    same = all(torch.equal(r, i) for r, i in zip(ref, imgs))
+    del g
+    b.close()
+    # the plain estimator on the first eight scenes at 1 spp
+    pr = 0
+    e0, e1 = events()
+    e0.record(stream)
+    for c, p, (w, h), a, i in list(zip(ctxs, params, sizes, accs, imgs))[:8]:
+        q = copy.copy(p)
+        q.spp = 1
+        q.flags &= ~aarbf.FLAG_MAJORANT_TRACKING
+        c.render(q, w, h, a, i, stream=sp)
+        pr += w * h
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_plain = e0.elapsed_time(e1)
+    for c in ctxs:
+        c.close()
+    return {"scenes": len(ctxs), "particles": particles, "rays": rays,
+            "sequential_ms": t_seq, "sequential_mrays_s": rays / t_seq / 1e3,
+            "batched_direct_ms": t_direct, "batched_graph_ms": t_graph, "batched_mrays_s": rays / t_graph / 1e3,
+            "speedup_vs_sequential": t_seq / t_graph, "images_identical": bool(same),
+            "autotuned": {"candidate_cap": cap, "stage_bins": bins,
+                          "proxy_ms": {f"{k[0]}/{k[1]}": round(v, 3) for k, v in table.items()}},
+            "plain_estimator_mrays_s": pr / t_plain / 1e3, "plain_sample": "first 8 scenes, 1 spp",
+            "speedup_vs_plain": (rays / t_graph) / (pr / t_plain)}
 
 
 def variant_timings(ctx, args, dom, rmax, accum, image, stream):
@@ -491,6 +739,9 @@ def main():
                "steps": k_e2e, "ms_per_step": te / k_e2e * 1e3}
 
     variants = None if args.no_variants else variant_timings(ctx, args, dom, rmax, accum, image, stream)
+    diff = differentiable_timing(args, dev, stream) if args.diff_views > 0 and world == 1 else None
+    batched = batched_timing(args, dev, stream) if args.batch_scenes > 0 and world == 1 else None
+    precision = precision_timing(args, dev, stream) if args.precision_particles > 0 and world == 1 else None
 
     cpu = None
     rmse = None
@@ -523,6 +774,7 @@ def main():
                          "accumulate_ms": accumulate_ms / max(timed_renders, 1), "kernel_counters": counts},
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": 2 * timed_renders,
             "build_ms": build_s * 1e3, "plain_estimator": plain, "variants": variants, "equal_rmse": rmse,
+            "differentiable": diff, "batched": batched, "precision": precision,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

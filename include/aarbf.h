@@ -182,6 +182,35 @@ aarbf_status aarbf_render_count(aarbf_ctx *ctx, const aarbf_params *p, int width
 aarbf_status aarbf_set_kernel_timing(aarbf_ctx *ctx, int enable);
 aarbf_status aarbf_get_kernel_times(aarbf_ctx *ctx, double *render_ms, double *accumulate_ms,
                                     uint32_t *renders);
+/* ---- FP16 storage form (no counterpart in the reference) -------------------------------- */
+
+/* Storage of the scene the next aarbf_build makes. AARBF_STORAGE_FP16: positions as FP16
+ * offsets from the centre of each run of 256 Hilbert-sorted particles (fp32 centre per run),
+ * attribute and per-particle colour weights in FP16, radii fp32; the tracking kernels read the
+ * packed records. Results are exact for the rounded scene (every kernel sees the same decoded
+ * values); the rounding itself changes the image slightly. */
+enum { AARBF_STORAGE_FP32 = 0, AARBF_STORAGE_FP16 = 1 };
+aarbf_status aarbf_set_storage(aarbf_ctx *ctx, int format);
+
+/* ---- batched rendering (no counterpart in the reference) -------------------------------- */
+
+/* Many scenes, views and resolutions in one persistent launch of the ray-per-warp kernel plus
+ * one accumulation launch. aarbf_batch_create binds nscenes contexts (each with its own built
+ * scene and transfer functions, all on one device), their parameters (majorant tracking with
+ * AARBF_TRAVERSAL_AUTO; per-scene frame, spp, camera, stage_bins), resolutions and caller-owned
+ * framebuffers, reserves every scene's working memory and uploads the launch blocks
+ * (synchronous). aarbf_batch_render then only enqueues the two kernels on `stream`: it allocates
+ * nothing and does not synchronise, so it can be called repeatedly or captured; candidate_cap
+ * (0, 256, 512, 1024) picks the staging-buffer depth. Results equal aarbf_render of each scene.
+ * The contexts must outlive the batch and not be rebuilt while it is used. */
+typedef struct aarbf_batch aarbf_batch;
+aarbf_status aarbf_batch_create(aarbf_batch **out, aarbf_ctx *const *ctxs, const aarbf_params *params,
+                                int nscenes, const int *widths, const int *heights,
+                                float *const *accums, float *const *images);
+aarbf_status aarbf_batch_render(aarbf_batch *batch, int candidate_cap, void *stream);
+aarbf_status aarbf_batch_destroy(aarbf_batch *batch);
+const char *aarbf_batch_last_error(const aarbf_batch *batch);
+
 /* ---- differentiable form (no counterpart in the reference) ------------------------------- */
 
 /* Expected stochastic marching: the reference's stochasticMarching (deviceCodeRBF.hlsl:67-139)

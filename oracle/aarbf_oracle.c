@@ -429,6 +429,58 @@ static float *dupf(const float *src, size_t cnt) {
   return d;
 }
 
+/* ---- FP16 storage form (no counterpart in the reference) ---------------------------------- */
+
+uint16_t orc_f2h(float f) {
+  uint32_t x = f2u(f);
+  uint32_t sign = (x >> 16) & 0x8000u, ax = x & 0x7fffffffu;
+  if (ax >= 0x7f800000u) return (uint16_t)(sign | (ax > 0x7f800000u ? 0x7e00u : 0x7c00u));
+  if (ax >= 0x477ff000u) return (uint16_t)(sign | 0x7c00u); /* >= 65520 rounds to infinity */
+  if (ax <= 0x33000000u) return (uint16_t)sign;            /* <= 2^-25 rounds to zero (tie to even) */
+  int e = (int)(ax >> 23) - 127;
+  uint32_t mant = (ax & 0x7fffffu) | 0x800000u;
+  int shift = e < -14 ? -e - 1 : 13; /* bits dropped: subnormal results keep fewer */
+  uint32_t q = mant >> shift, rem = mant & ((1u << shift) - 1u), halfway = 1u << (shift - 1);
+  if (rem > halfway || (rem == halfway && (q & 1u))) ++q;
+  if (e < -14) return (uint16_t)(sign | q); /* q == 0x400 is the smallest normal, encoded alike */
+  return (uint16_t)(sign | (((uint32_t)(e + 15) << 10) + (q - 0x400u)));
+}
+
+float orc_h2f(uint16_t h) {
+  uint32_t sign = (uint32_t)(h & 0x8000u) << 16, e = (h >> 10) & 0x1fu, m = h & 0x3ffu;
+  if (e == 0x1f) return u2f(sign | 0x7f800000u | (m << 13));
+  if (e == 0) {
+    float v = (float)m * 0x1p-24f; /* exact */
+    return sign ? -v : v;
+  }
+  return u2f(sign | ((e + 112u) << 23) | (m << 13));
+}
+
+#define ORC_FP16_RUN 256 /* particles sharing one fp32 origin */
+
+/* positions relative to the centre of their run's bounding box, and the attribute, through FP16 */
+static void quantize_positions(orc_scene *s) {
+  for (uint64_t b = 0; b < s->n; b += ORC_FP16_RUN) {
+    uint64_t e = b + ORC_FP16_RUN < s->n ? b + ORC_FP16_RUN : s->n;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint64_t i = b; i < e; ++i)
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = fminf(lo[a], s->xyzw[4 * i + a]);
+        hi[a] = fmaxf(hi[a], s->xyzw[4 * i + a]);
+      }
+    float o[3];
+    for (int a = 0; a < 3; ++a) o[a] = (lo[a] + hi[a]) * 0.5f;
+    for (uint64_t i = b; i < e; ++i) {
+      for (int a = 0; a < 3; ++a) s->xyzw[4 * i + a] = o[a] + orc_h2f(orc_f2h(s->xyzw[4 * i + a] - o[a]));
+      s->xyzw[4 * i + 3] = orc_h2f(orc_f2h(s->xyzw[4 * i + 3]));
+    }
+  }
+}
+
+static void quantize_weights(orc_scene *s) {
+  for (uint64_t i = 0; i < 4 * s->n; ++i) s->w4[i] = orc_h2f(orc_f2h(s->w4[i]));
+}
+
 /* deviceCodeRBF.hlsl:349-351 (radius), :366-376 (colour weights), deviceCodeBounds.hlsl:59-65 */
 static void prepass(orc_scene *s, const float *radii, const orc_tf_desc *tf) {
   for (uint64_t i = 0; i < s->n; ++i) {
@@ -581,7 +633,9 @@ orc_scene *orc_scene_create(const float *xyzw, const float *radii, const uint64_
   s->nc = tf->nc;
   s->density = dupf(tf->density, (size_t)tf->nd);
   s->nd = tf->nd;
+  if (tf->storage_fp16) quantize_positions(s);
   prepass(s, radii, tf);
+  if (tf->storage_fp16) quantize_weights(s);
   for (uint32_t l = 0; l < s->nleaves; ++l) s->leaf_key[l] = keys[(uint64_t)l * s->ppl];
   leaf_bounds(s);
   if (s->nleaves == 0) {
@@ -620,6 +674,8 @@ void orc_scene_get_bvh(const orc_scene *s, uint32_t *left, uint32_t *right, floa
   if (leaf_eff) memcpy(leaf_eff, s->leaf_eff, 6 * (size_t)s->nleaves * sizeof(float));
   if (root_box) memcpy(root_box, s->root_box, 6 * sizeof(float));
 }
+
+void orc_scene_get_particles(const orc_scene *s, float *xyzw) { memcpy(xyzw, s->xyzw, 16 * s->n); }
 
 void orc_scene_get_prepass(const orc_scene *s, float *rec0, float *w4, float *rgeom) {
   if (rec0) memcpy(rec0, s->rec0, 4 * s->n * sizeof(float));

@@ -68,7 +68,14 @@ typedef struct orc_tf_desc {
   const float *radius; int nr;   /* R table */
   const float *density; int nd;  /* R table */
   float alpha_floor;             /* opacity below this counts as transparent (0: only alpha == 0) */
+  int storage_fp16;              /* scene option: positions (relative to the centre of each run of
+                                    256 sorted particles), attributes and the per-particle weights
+                                    a^3, rgb^2.2 a^3 are rounded to FP16 */
 } orc_tf_desc;
+
+/* IEEE binary16 conversions: round to nearest even, and exact widening */
+uint16_t orc_f2h(float f);
+float orc_h2f(uint16_t h);
 
 /* xyzw: Hilbert-sorted particles with normalised attribute; radii may be NULL.
  * keys: Hilbert keys of the sorted particles. */
@@ -82,6 +89,8 @@ uint32_t orc_scene_num_leaves(const orc_scene *s);
 void orc_scene_get_bvh(const orc_scene *s, uint32_t *left, uint32_t *right, float *node_box,
                        float *leaf_box, float *leaf_eff, float *root_box);
 void orc_scene_get_prepass(const orc_scene *s, float *rec0, float *w4, float *rgeom);
+/* the scene's sorted particles as rendered (after FP16 rounding in the FP16 storage form) */
+void orc_scene_get_particles(const orc_scene *s, float *xyzw);
 
 /* point query at x: returns hit count; acc = {D, R, G, B} fixed point (2^-40 units) */
 int orc_point_query(const orc_scene *s, const float *x, int64_t *acc);

@@ -43,7 +43,7 @@ class OrcParams(ctypes.Structure):
 class OrcTF(ctypes.Structure):
     _fields_ = [("color", ctypes.c_void_p), ("nc", ctypes.c_int), ("radius", ctypes.c_void_p),
                 ("nr", ctypes.c_int), ("density", ctypes.c_void_p), ("nd", ctypes.c_int),
-                ("alpha_floor", ctypes.c_float)]
+                ("alpha_floor", ctypes.c_float), ("storage_fp16", ctypes.c_int)]
 
 
 def build():
@@ -82,6 +82,7 @@ def lib():
             "orc_scene_num_leaves": ([P], u32),
             "orc_scene_get_bvh": ([P, P, P, P, P, P, P], None),
             "orc_scene_get_prepass": ([P, P, P, P], None),
+            "orc_scene_get_particles": ([P, P], None),
             "orc_point_query": ([P, P, P], i32),
             "orc_point_query_brute": ([P, P, P], i32),
             "orc_render": ([P, ctypes.POINTER(OrcParams), i32, i32, P, P, i32], None),
@@ -89,6 +90,7 @@ def lib():
             "orc_render_splat": ([P, ctypes.POINTER(OrcParams), i32, i32, P, i32], None),
             "orc_taa": ([P, P, P, P, i32, i32, i32], None),
             "orc_set_threads": ([i32], None),
+            "orc_f2h": ([f32], ctypes.c_uint16), "orc_h2f": ([ctypes.c_uint16], f32),
             "orc_diff_forward": ([P, P, i32, i32, i32, P, i32], ctypes.c_double),
             "orc_diff_backward": ([P, P, i32, i32, i32, P, P, P, P, P, i32], None),
             "orc_render_f64": ([P, ctypes.POINTER(OrcParams), i32, i32, i32, i32, i32, i32, i32, i32, u64, P, i32],
@@ -161,7 +163,7 @@ def tf_from_rgba8(cm, rm, dm):
 class Scene:
     """Prepass + leaf bounds + LBVH of Hilbert-sorted particles (as aarbf_build leaves them)."""
 
-    def __init__(self, sorted_xyzw, sorted_radii, keys, ppl, rbf_radius, tf, alpha_floor=0.0):
+    def __init__(self, sorted_xyzw, sorted_radii, keys, ppl, rbf_radius, tf, alpha_floor=0.0, fp16=False):
         self.xyzw = np.ascontiguousarray(sorted_xyzw, np.float32)
         self.radii = None if sorted_radii is None else np.ascontiguousarray(sorted_radii, np.float32)
         self.keys = np.ascontiguousarray(keys, np.uint64)
@@ -170,7 +172,8 @@ class Scene:
                            np.ascontiguousarray(rm, np.float32).reshape(-1),
                            np.ascontiguousarray(dm, np.float32).reshape(-1))
         c, r, d = self._tf_arrays
-        t = OrcTF(c.ctypes.data, len(c), r.ctypes.data, len(r), d.ctypes.data, len(d), float(alpha_floor))
+        t = OrcTF(c.ctypes.data, len(c), r.ctypes.data, len(r), d.ctypes.data, len(d), float(alpha_floor),
+                  int(bool(fp16)))
         self.n = len(self.xyzw)
         self.h = lib().orc_scene_create(_p(self.xyzw), _p(self.radii), _p(self.keys), self.n, int(ppl),
                                         float(rbf_radius), ctypes.byref(t))
@@ -191,6 +194,12 @@ class Scene:
         rb = np.zeros(6, np.float32)
         lib().orc_scene_get_bvh(self.h, _p(left), _p(right), _p(nb), _p(lb), _p(le), _p(rb))
         return left, right, nb, lb, le, rb
+
+    def particles(self):
+        out = np.zeros((self.n, 4), np.float32)
+        if self.n:
+            lib().orc_scene_get_particles(self.h, _p(out))
+        return out
 
     def prepass(self):
         rec0 = np.zeros((self.n, 4), np.float32)
@@ -266,13 +275,13 @@ def diff_backward(pos, radius, attr, tf, views, w, h, grad_images, threads=0):
     return gp, gr, ga, gt
 
 
-def build_scene(xyzw, radii, dom, ppl, rbf_radius, tf, alpha_floor=0.0):
+def build_scene(xyzw, radii, dom, ppl, rbf_radius, tf, alpha_floor=0.0, fp16=False):
     """The whole build pipeline on the CPU: keys, sort, gather/normalise, scene."""
     xyzw = np.ascontiguousarray(xyzw, np.float32)
     keys = hilbert_keys(xyzw, dom)
     perm = sort_perm(keys, xyzw)
     sx, sr = gather_normalize(xyzw, radii, perm, dom[6], dom[7])
-    return Scene(sx, sr, keys[perm], ppl, rbf_radius, tf, alpha_floor), keys[perm], perm
+    return Scene(sx, sr, keys[perm], ppl, rbf_radius, tf, alpha_floor, fp16), keys[perm], perm
 
 
 def taa(image, prev, disable=False):

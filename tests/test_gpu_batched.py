@@ -1,0 +1,73 @@
+"""Batched rendering (aarbf_batch_create / aarbf_batch_render): several scenes of different
+sizes, resolutions and spp in one persistent launch give the same bits as one aarbf_render per
+scene, also when the launch is replayed from a CUDA graph."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _scenes(aarbf_mod):
+    from aarbf import scenes
+    rng = np.random.default_rng(11)
+    out = []
+    for k, (n, w, h, spp) in enumerate([(3000, 24, 16, 1), (20000, 40, 30, 3), (8000, 16, 16, 2), (50000, 32, 24, 4)]):
+        sc = scenes.config_clusters(n, clusters=4 + k, seed=20 + k)
+        cm, rm, dm = scenes.tf_four_peaks(64, seed=k)
+        dom = np.concatenate([sc.xyzw[:, :3].min(0), sc.xyzw[:, :3].max(0),
+                              [sc.xyzw[:, 3].min(), sc.xyzw[:, 3].max()]]).astype(np.float32)
+        ctx = aarbf_mod.Context(0)
+        ctx.set_domain(dom)
+        ctx.set_transfer_functions_f32(cm, rm, dm)
+        ctx.set_opacity_floor(1 / 255)
+        ctx.set_particles(sc.xyzw, sc.radii)
+        ctx.build(float(sc.radii.max()), 4)
+        cam = scenes.orbit_camera(azimuth_deg=float(rng.uniform(0, 360)), elevation_deg=float(rng.uniform(-30, 30)))
+        rp = scenes.native_params(cam, w, h, float(sc.radii.max()), 0.002, 300.0, dom, spp=spp, frame_id=5 * k,
+                                  majorant=True, bin_length=0.008)
+        out.append((ctx, rp, (w, h)))
+    return out
+
+
+def test_batched_matches_single_renders(aarbf_mod):
+    import torch
+    items = _scenes(aarbf_mod)
+    ref = []
+    for ctx, rp, (w, h) in items:
+        acc = torch.zeros((h, w, 4), device="cuda")
+        img = torch.zeros_like(acc)
+        ctx.render(rp, w, h, acc, img)
+        ctx.sync()
+        ref.append((acc.cpu().numpy(), img.cpu().numpy()))
+    assert any((r[1][..., :3] > 0).mean() > 0.01 for r in ref)
+    accs = [torch.zeros((h, w, 4), device="cuda") for _, _, (w, h) in items]
+    imgs = [torch.zeros_like(a) for a in accs]
+    b = aarbf_mod.Batch([c for c, _, _ in items], [p for _, p, _ in items], [s for _, _, s in items], accs, imgs)
+    for cap in (0, 512, 1024):
+        for a in accs:
+            a.zero_()
+        b.render(cap)
+        torch.cuda.synchronize()
+        for (ra, ri), a, i in zip(ref, accs, imgs):
+            assert np.array_equal(a.cpu().numpy().view(np.uint32), ra.view(np.uint32))
+            assert np.array_equal(i.cpu().numpy().view(np.uint32), ri.view(np.uint32))
+    # the same launch replayed from a CUDA graph
+    st = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        b.render(0, st)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=st):
+        b.render(0, st)
+    for a, i in zip(accs, imgs):
+        a.zero_()
+        i.zero_()
+    torch.cuda.synchronize()
+    g.replay()
+    torch.cuda.synchronize()
+    for (ra, ri), a, i in zip(ref, accs, imgs):
+        assert np.array_equal(i.cpu().numpy().view(np.uint32), ri.view(np.uint32))
+    del g
+    b.close()
+    for ctx, _, _ in items:
+        ctx.close()

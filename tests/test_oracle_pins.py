@@ -258,3 +258,24 @@ def test_diff_adjoint_matches_finite_differences(orc):
     cos = an @ fd / (np.linalg.norm(an) * np.linalg.norm(fd))
     assert cos > 0.999
     assert np.linalg.norm(an - fd) < 0.03 * np.linalg.norm(fd)
+
+
+def test_fp16_conversion_matches_ieee(orc):
+    """the oracle's float -> half rounding (nearest, ties to even) and widening agree with IEEE
+    binary16 (numpy's float16) on every half value, random floats over 13 decades, values next
+    to halfway points, overflow, underflow and the specials"""
+    L = orc.lib()
+    for h in range(0, 65536, 7):
+        ref = np.array([h], np.uint16).view(np.float16)[0]
+        f = L.orc_h2f(h)
+        assert (np.isnan(ref) and math.isnan(f)) or np.float32(ref) == np.float32(f)
+    rng = np.random.default_rng(4)
+    xs = np.concatenate([rng.normal(0, s, 4000) for s in (1e-8, 1e-6, 1e-4, 1e-2, 1, 100, 1e4, 1e5)])
+    hw = (np.float16(rng.normal(0, 1, 500)).astype(np.float32) + np.float16(rng.normal(0, 1, 500)).astype(np.float32)) / 2
+    xs = np.concatenate([xs, hw, np.nextafter(hw, np.float32(9)), np.nextafter(hw, np.float32(-9)),
+                         [65504, 65519.99, 65520, 2 ** -25, 2 ** -24, 3 * 2 ** -26, 0.0, -0.0, np.inf, -np.inf]])
+    xs = xs.astype(np.float32)
+    with np.errstate(over="ignore"):
+        want = xs.astype(np.float16).view(np.uint16)
+    got = np.array([L.orc_f2h(float(x)) for x in xs], np.uint16)
+    assert np.array_equal(got, want)
