@@ -113,12 +113,35 @@ cudaError_t launch_refit(const float4* rec0, const float* rgeom, uint64_t n, uin
                          uint32_t nleaves, Node* nodes, Node* nodes_ref, const uint32_t* leaf_parent,
                          uint32_t* counters, float* leaf_box, float* leaf_eff, float* root_box,
                          cudaStream_t st);
+// the tracking kernels, built for the fp32 records (r32) and the FP16 storage form (r16)
+struct BatchArgs;
+#define AARBF_RENDER_DECLS                                                                      \
+  cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st, const cudaEvent_t* marks); \
+  bool render_uses_warp_kernel(const RenderLaunch& L);                                          \
+  cudaError_t render_warp_stack_words(size_t* words);                                           \
+  cudaError_t launch_render_batched(const BatchArgs& B, cudaStream_t st);
+namespace r32 { AARBF_RENDER_DECLS }
+namespace r16 { AARBF_RENDER_DECLS }
+#undef AARBF_RENDER_DECLS
+
 // marks (optional): three events recorded before the tracking kernel, between it and the
 // accumulation pass, and after the accumulation pass.
-cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st, const cudaEvent_t* marks = nullptr);
-bool render_uses_warp_kernel(const RenderLaunch& L);
-cudaError_t render_warp_stack_words(size_t* words);
-cudaError_t launch_splat(const RenderLaunch& L, cudaStream_t st);
+inline cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st, const cudaEvent_t* marks = nullptr) {
+  return L.s.posq ? r16::launch_render(L, st, marks) : r32::launch_render(L, st, marks);
+}
+inline bool render_uses_warp_kernel(const RenderLaunch& L) { return r32::render_uses_warp_kernel(L); }
+// stack words for the largest grid of either build
+inline cudaError_t render_warp_stack_words(size_t* words) {
+  size_t a = 0, b = 0;
+  cudaError_t e = r32::render_warp_stack_words(&a);
+  if (e == cudaSuccess) e = r16::render_warp_stack_words(&b);
+  *words = a > b ? a : b;
+  return e;
+}
+// slabs: the splat slab starts (nslabs entries, the last beyond every ray's exit) for the
+// ray-per-warp splat kernel; NULL selects the thread-per-pixel kernel
+cudaError_t launch_splat(const RenderLaunch& L, cudaStream_t st, const float* slabs = nullptr, int nslabs = 0);
+size_t splat_stack_words();
 
 // several scenes in one persistent launch of the ray-per-warp kernel (render.cu)
 struct BatchArgs {
@@ -130,8 +153,11 @@ struct BatchArgs {
   int candidate_cap;
   unsigned long long* work_counter;
   uint32_t* warp_stacks;
+  bool fp16;                     // every scene is in the FP16 storage form
 };
-cudaError_t launch_render_batched(const BatchArgs& B, cudaStream_t st);
+inline cudaError_t launch_render_batched(const BatchArgs& B, cudaStream_t st) {
+  return B.fp16 ? r16::launch_render_batched(B, st) : r32::launch_render_batched(B, st);
+}
 
 // FP16 storage form (fp16.cu)
 cudaError_t launch_quantize_positions(float4* xyzw, uint64_t n, uint2* posq, float4* origin, cudaStream_t st);
@@ -198,6 +224,9 @@ struct aarbf_ctx {
   // status word, persistent-kernel work counter, per-sample colour planes
   aarbf::DevBuf status, work, samples, noise_buf, warp_stacks;
   float max_radius = 0.0f;
+  aarbf::DevBuf splat_slabs;      // slab starts of the splat kernel, for splat_spacing
+  float splat_spacing = 0.0f;
+  int splat_nslabs = 0;
   bool storage_fp16 = false;     // FP16 storage form (takes effect at the next build)
   bool built_fp16 = false;       // the built scene is in the FP16 form
   aarbf::DevBuf posq, colq, origin, reval;

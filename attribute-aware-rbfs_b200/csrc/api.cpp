@@ -333,7 +333,7 @@ aarbf_status aarbf_destroy(aarbf_ctx* ctx) {
                     &ctx->sorted_keys, &ctx->tf_color, &ctx->tf_radius, &ctx->tf_density, &ctx->noise,
                     &ctx->fb_accum, &ctx->fb_image, &ctx->status, &ctx->work, &ctx->samples,
                     &ctx->noise_buf, &ctx->warp_stacks, &ctx->diff_views, &ctx->diff_ckpt, &ctx->diff_grad,
-                    &ctx->posq, &ctx->colq, &ctx->origin, &ctx->reval};
+                    &ctx->posq, &ctx->colq, &ctx->origin, &ctx->reval, &ctx->splat_slabs};
   for (DevBuf* b : bufs) b->release();
   for (auto* v : {&ctx->ev_pending, &ctx->ev_free})
     for (auto& ev : *v)
@@ -721,6 +721,7 @@ struct aarbf_batch {
   uint64_t total_pixels = 0;
   DevBuf dev;           // launch blocks, item and pixel prefix sums, work counter
   uint32_t* warp_stacks = nullptr;
+  bool fp16 = false;
   std::string last_error;
 };
 
@@ -738,6 +739,8 @@ aarbf_status aarbf_batch_create(aarbf_batch** out, aarbf_ctx* const* ctxs, const
     aarbf_ctx* ctx = ctxs[i];
     if (!ctx || ctx->device != c0->device)
       return fail(c0, AARBF_ERR_INVALID_ARGUMENT, "batched scenes need contexts on one device");
+    if (ctx->built_fp16 != c0->built_fp16)
+      return fail(c0, AARBF_ERR_UNSUPPORTED, "batched scenes need one storage form");
     if (!accums[i] || !images[i]) return fail(c0, AARBF_ERR_INVALID_ARGUMENT, "batched scenes need framebuffers");
     const aarbf_params& p = params[i];
     if (!(p.flags & kFlagMajorantTracking) || (p.flags & kFlagBlueNoise) || p.traversal != AARBF_TRAVERSAL_AUTO)
@@ -762,6 +765,7 @@ aarbf_status aarbf_batch_create(aarbf_batch** out, aarbf_ctx* const* ctxs, const
   b->nscenes = nscenes;
   b->total_pixels = pix.back();
   b->warp_stacks = c0->warp_stacks.as<uint32_t>();
+  b->fp16 = c0->built_fp16;
   const size_t lb = sizeof(RenderLaunch) * (size_t)nscenes, ob = sizeof(uint64_t) * ((size_t)nscenes + 1);
   const size_t off_items = (lb + 255) / 256 * 256, off_pix = off_items + (ob + 255) / 256 * 256;
   const size_t off_ctr = off_pix + (ob + 255) / 256 * 256;
@@ -799,6 +803,7 @@ aarbf_status aarbf_batch_render(aarbf_batch* b, int candidate_cap, void* stream)
   B.candidate_cap = candidate_cap;
   B.work_counter = reinterpret_cast<unsigned long long*>(base + off_ctr);
   B.warp_stacks = b->warp_stacks;
+  B.fp16 = b->fp16;
   cudaError_t e = launch_render_batched(B, (cudaStream_t)stream);
   if (e != cudaSuccess) {
     b->last_error = std::string("batch render: ") + cudaGetErrorString(e);
@@ -932,7 +937,56 @@ aarbf_status aarbf_render_splat(aarbf_ctx* ctx, const aarbf_params* p, int w, in
   RenderLaunch L;
   aarbf_status s = fill_launch(ctx, p, w, h, nullptr, image, L);
   if (s != AARBF_OK) return s;
-  CK(launch_splat(L, (cudaStream_t)stream), "splat launch");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (p->traversal == AARBF_TRAVERSAL_THREAD) {
+    CK(launch_splat(L, st), "splat launch");
+    return AARBF_OK;
+  }
+  // slab starts of the ray-per-warp kernel: the running sum t += spacing from 0, tabulated until
+  // it passes the farthest corner of the padded box (every ray's exit lies before it)
+  const float spacing = (float)(15 / 8) * p->unit;
+  double far2 = 0.0;
+  for (int c = 0; c < 8; ++c) {
+    double d2 = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      double v = ((c >> a) & 1) ? (double)p->aabb_max[a] + p->rbf_radius : (double)p->aabb_min[a] - p->rbf_radius;
+      d2 += (v - p->cam_pos[a]) * (v - p->cam_pos[a]);
+    }
+    far2 = std::fmax(far2, d2);
+  }
+  const float tfar = (float)(std::sqrt(far2) * 1.001) + 2.0f * spacing;
+  std::vector<float> tab;
+  bool ok = spacing > 0.0f && std::isfinite(tfar);
+  if (ok) {
+    float t = 0.0f;
+    tab.push_back(t);
+    while (t < tfar) {
+      const float nt = t + spacing;
+      if (!(nt > t) || tab.size() >= (1u << 20)) {
+        ok = false;
+        break;
+      }
+      t = nt;
+      tab.push_back(t);
+    }
+  }
+  if (!ok) {  // too many slabs for the table: thread-per-pixel kernel
+    CK(launch_splat(L, st), "splat launch");
+    return AARBF_OK;
+  }
+  if (ctx->splat_spacing != spacing || ctx->splat_nslabs < (int)tab.size()) {
+    CK(ctx->splat_slabs.reserve(sizeof(float) * tab.size()), "slab table alloc");
+    CK(cudaMemcpyAsync(ctx->splat_slabs.ptr, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice, st),
+       "slab table upload");
+    CK(cudaStreamSynchronize(st), "slab table upload");
+    ctx->splat_spacing = spacing;
+    ctx->splat_nslabs = (int)tab.size();
+  }
+  if (!ctx->work.ptr) CK(ctx->work.reserve(256), "work counter");
+  L.work_counter = ctx->work.as<uint32_t>();
+  CK(ctx->warp_stacks.reserve(4 * splat_stack_words()), "warp stacks");
+  L.warp_stacks = ctx->warp_stacks.as<uint32_t>();
+  CK(launch_splat(L, st, ctx->splat_slabs.as<float>(), ctx->splat_nslabs), "splat launch");
   return AARBF_OK;
 }
 

@@ -15,7 +15,17 @@
 #include "aarbf_internal.h"
 #include "warp_traverse.cuh"
 
+// Compiled twice: AARBF_RENDER_NS = r32 reads the fp32 prepass records, r16 the packed FP16
+// storage form (AARBF_FP16_RECORDS); each build has no branch on the format in its hot loops.
+#ifndef AARBF_RENDER_NS
+#define AARBF_RENDER_NS r32
+#endif
+#ifndef AARBF_FP16_RECORDS
+#define AARBF_FP16_RECORDS 0
+#endif
+
 namespace aarbf {
+namespace AARBF_RENDER_NS {
 
 namespace {
 
@@ -30,28 +40,29 @@ __device__ __forceinline__ void ctr_add(unsigned long long* c, int i, unsigned l
   if (c) atomicAdd(c + i, v);
 }
 
-// Particle records: the fp32 prepass arrays, or the packed FP16 storage form (fp16.cu) when the
-// scene has one; both decode to the same floats.
+// Particle records: the fp32 prepass arrays, or the packed FP16 storage form (fp16.cu); both
+// decode to the same floats.
+#if AARBF_FP16_RECORDS
 __device__ __forceinline__ float hval16(uint32_t b) { return __half2float(__ushort_as_half((unsigned short)b)); }
 
 __device__ __forceinline__ float4 part_rec(const SceneView& s, uint32_t i) {
-  if (!s.posq) return __ldg(s.rec0 + i);
   const uint2 q = __ldg(s.posq + i);
   const float4 o = __ldg(s.origin + (i >> 8));
   return make_float4(o.x + hval16(q.x & 0xffffu), o.y + hval16(q.x >> 16), o.z + hval16(q.y & 0xffffu),
                      __ldg(s.reval + i));
 }
 
-__device__ __forceinline__ float part_a3(const SceneView& s, uint32_t i) {
-  if (!s.posq) return __ldg(&s.w4[i].x);
-  return hval16(__ldg(&s.posq[i].y) >> 16);
-}
+__device__ __forceinline__ float part_a3(const SceneView& s, uint32_t i) { return hval16(__ldg(&s.posq[i].y) >> 16); }
 
 __device__ __forceinline__ float4 part_w(const SceneView& s, uint32_t i) {
-  if (!s.posq) return __ldg(s.w4 + i);
   const uint2 c = __ldg(s.colq + i);
   return make_float4(part_a3(s, i), hval16(c.x & 0xffffu), hval16(c.x >> 16), hval16(c.y & 0xffffu));
 }
+#else
+__device__ __forceinline__ float4 part_rec(const SceneView& s, uint32_t i) { return __ldg(s.rec0 + i); }
+__device__ __forceinline__ float part_a3(const SceneView& s, uint32_t i) { return __ldg(&s.w4[i].x); }
+__device__ __forceinline__ float4 part_w(const SceneView& s, uint32_t i) { return __ldg(s.w4 + i); }
+#endif
 
 struct Sample {
   int count;
@@ -786,6 +797,15 @@ __device__ float4 raygen_sample(const RenderLaunch& L, uint32_t frame, int px, i
 // ============================================================================================
 
 constexpr int kWarpsPerBlock = 4;
+// resident blocks per SM the ray-per-warp kernels are compiled for (caps registers at
+// 65536 / (128 * kWarpMinBlocks)); the tracker is out of line unless AARBF_TRACK_INLINE
+#ifndef AARBF_WARP_MIN_BLOCKS
+#define AARBF_WARP_MIN_BLOCKS 8
+#endif
+#ifndef AARBF_TRACK_INLINE
+#define AARBF_TRACK_INLINE 0
+#endif
+constexpr int kWarpMinBlocks = AARBF_WARP_MIN_BLOCKS;
 
 // per-warp shared memory: staged candidates, then per-bin lists of candidate slots (CSR)
 template <int CAPW>
@@ -1165,7 +1185,12 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
 }
 
 template <int CAPW>
-__device__ __noinline__ void track_majorant_warp(const RenderLaunch& L, Tracker& tr_io, const Ray& ray_io,
+#if AARBF_TRACK_INLINE
+__device__ __forceinline__
+#else
+__device__ __noinline__
+#endif
+void track_majorant_warp(const RenderLaunch& L, Tracker& tr_io, const Ray& ray_io,
                                                  WarpBuf<CAPW>* buf, uint32_t* stk) {
   Tracker tr = tr_io;
   const Ray ray = ray_io;
@@ -1208,7 +1233,7 @@ __device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t
 }
 
 template <int CAPW>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_render_warp(const __grid_constant__ RenderLaunch L) {
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks) k_render_warp(const __grid_constant__ RenderLaunch L) {
   extern __shared__ __align__(16) char smem[];
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
   WarpBuf<CAPW>* buf = reinterpret_cast<WarpBuf<CAPW>*>(smem) + wib;
@@ -1226,7 +1251,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_render_warp(const __
 // Several scenes in one persistent launch: Ls[s] is scene s's launch block, items
 // [item_ofs[s], item_ofs[s + 1]) are its work items; warps take items from one counter.
 template <int CAPW>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 8)
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks)
     k_render_warp_batched(const RenderLaunch* __restrict__ Ls, const uint64_t* __restrict__ item_ofs, int nscenes,
                           unsigned long long* work_counter, uint32_t* warp_stacks) {
   extern __shared__ __align__(16) char smem[];
@@ -1459,7 +1484,7 @@ cudaError_t launch_render_batched(const BatchArgs& B, cudaStream_t st) {
 
 cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st, const cudaEvent_t* marks) {
   if (L.width <= 0 || L.height <= 0) return cudaSuccess;
-  if (render_uses_warp_kernel(L)) {
+  if (AARBF_RENDER_NS::render_uses_warp_kernel(L)) {
     switch (L.candidate_cap) {
       case 512: return launch_warp<512>(L, st, marks);
       case 1024: return launch_warp<1024>(L, st, marks);
@@ -1474,4 +1499,5 @@ cudaError_t launch_render(const RenderLaunch& L, cudaStream_t st, const cudaEven
   }
 }
 
+}  // namespace AARBF_RENDER_NS
 }  // namespace aarbf

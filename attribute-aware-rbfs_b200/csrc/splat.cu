@@ -7,6 +7,7 @@
 // a run of slabs are staged once per BVH traversal in shared memory and sorted; a slab with more
 // than the buffer holds is resolved by a streaming top-15 traversal of that slab alone.
 #include "aarbf_internal.h"
+#include "warp_traverse.cuh"
 
 namespace aarbf {
 
@@ -15,16 +16,6 @@ namespace {
 constexpr int kBlock = 128;
 constexpr int kCap = 32;
 constexpr int kKeep = 15;  // PARTICLE_BUFFER_SIZE, deviceCodeSplat.hlsl:36
-
-__device__ __forceinline__ bool seg_box(float lx, float ly, float lz, float hx, float hy, float hz, float3 o,
-                                        float3 inv, float t0, float t1, float pad) {
-  float ax = (lx - pad - o.x) * inv.x, bx = (hx + pad - o.x) * inv.x;
-  float ay = (ly - pad - o.y) * inv.y, by = (hy + pad - o.y) * inv.y;
-  float az = (lz - pad - o.z) * inv.z, bz = (hz + pad - o.z) * inv.z;
-  float tn = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), t0));
-  float tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), t1));
-  return tn <= tf;
-}
 
 __device__ __forceinline__ float splat_radius(const RenderLaunch& L, uint32_t i) {
   float rg = __ldg(L.s.rgeom + i);
@@ -241,9 +232,237 @@ __global__ void __launch_bounds__(kBlock) k_splat(const RenderLaunch L, float pa
   L.image[(size_t)px + (size_t)L.width * (size_t)py] = res;
 }
 
+// ---- one warp per pixel --------------------------------------------------------------------
+// The slab starts are the reference's running sum t_{k+1} = t_k + spacing from t_0 = 0, the same
+// floats for every ray, so they are tabulated once per launch (slabs[]); a ray finds its first
+// slab by binary search. A run of slabs is staged by one warp-wide traversal of the
+// reference-bounds BVH (accepted samples with t in the run), sorted by (t, index) with a bitonic
+// network in shared memory, and then composited slab by slab (lanes shade the up to 15 samples
+// of a slab in parallel, the "over" chain runs in order); slabs without samples are skipped by a
+// binary search for the next sample's slab. A single slab with more samples than the buffer
+// takes its 15 smallest (t, index) by repeated minimum traversals.
+
+constexpr int kSplatWarps = 4;
+constexpr int kSplatCap = 512;
+
+struct SplatBuf {
+  float t[kSplatCap];
+  uint32_t id[kSplatCap];
+  uint32_t leaves[64];
+};
+
+struct SplatWarpArgs {
+  const float* slabs;  // slab starts, nslabs entries (the last one >= every ray's texit)
+  int nslabs;
+  float pad;
+  uint32_t* work_counter;
+  uint32_t* warp_stacks;
+};
+
+// first j in [lo, hi) with slabs[j] > x (hi if none)
+__device__ __forceinline__ int first_above(const float* slabs, int lo, int hi, float x) {
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (__ldg(slabs + mid) > x) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ void bitonic_sort(SplatBuf* b, int n, uint32_t lane) {
+  int P = 1;
+  while (P < n) P <<= 1;
+  for (int j = n + (int)lane; j < P; j += 32) {
+    b->t[j] = __int_as_float(0x7f800000);
+    b->id[j] = 0xffffffffu;
+  }
+  __syncwarp();
+  for (int size = 2; size <= P; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int p = (int)lane; p < P / 2; p += 32) {
+        const int a = 2 * p - (p & (stride - 1)), c = a + stride;
+        const bool up = (a & size) == 0;
+        const float ta = b->t[a], tc = b->t[c];
+        const uint32_t ia = b->id[a], ic = b->id[c];
+        if (less_ti(tc, ic, ta, ia) == up) {
+          b->t[a] = tc;
+          b->id[a] = ic;
+          b->t[c] = ta;
+          b->id[c] = ia;
+        }
+      }
+      __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(kSplatWarps * 32) k_splat_warp(const __grid_constant__ RenderLaunch L,
+                                                                 const SplatWarpArgs A) {
+  extern __shared__ __align__(16) char smem[];
+  const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, lt = lane_lt_mask();
+  SplatBuf* buf = reinterpret_cast<SplatBuf*>(smem) + wib;
+  uint32_t* stk = A.warp_stacks + ((size_t)blockIdx.x * kSplatWarps + wib) * kWarpStack;
+  const uint32_t total = (uint32_t)L.width * (uint32_t)L.height;
+  const float spacing = (float)(kKeep / 8) * L.unit;
+  const float atten = dexp(-L.unit * (float)(kKeep / 8));
+  const float3 rt = make_float3(L.aabb_max[0] + L.rbf_radius, L.aabb_max[1] + L.rbf_radius, L.aabb_max[2] + L.rbf_radius);
+  const float3 lb = make_float3(L.aabb_min[0] - L.rbf_radius, L.aabb_min[1] - L.rbf_radius, L.aabb_min[2] - L.rbf_radius);
+  const float3 o = make_float3(L.cam_pos[0], L.cam_pos[1], L.cam_pos[2]);
+  (void)spacing;
+  for (;;) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(A.work_counter, 1u);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= total) break;
+    const int px = (int)(item % (uint32_t)L.width), py = (int)(item / (uint32_t)L.width);
+    const float sx = ((float)px + 0.5f + L.jitter_x) / (float)L.width;
+    const float sy = ((float)py + 0.5f + L.jitter_y) / (float)L.height;
+    const float3 d = normalize3(make_float3((L.cam_d00[0] + sx * L.cam_du[0]) + sy * L.cam_dv[0],
+                                            (L.cam_d00[1] + sx * L.cam_du[1]) + sy * L.cam_dv[1],
+                                            (L.cam_d00[2] + sx * L.cam_du[2]) + sy * L.cam_dv[2]));
+    float tenter, texit;
+    aabb_clip(o, d, lb, rt, 0.0f, 10000.0f, tenter, texit);
+    float4 res = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (tenter < texit && L.s.nleaves > 0) {
+      const float3 inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+      // first slab whose end lies beyond the entry point
+      int k = first_above(A.slabs, 1, A.nslabs, tenter) - 1;
+      int run = 64;
+      for (int guard = 0; guard < (1 << 22) && k + 1 < A.nslabs; ++guard) {
+        const float ts = __ldg(A.slabs + k);
+        if (!(ts < texit) || res.w > 0.99f) break;
+        const int kend = min(k + run, A.nslabs - 1);
+        const float lo = fmaxf(tenter, ts), hi = fminf(texit, __ldg(A.slabs + kend));
+        int n = 0;
+        const bool ok = warp_traverse_nodes(
+            L.s, L.s.nodes_ref, stk, buf->leaves, L.status,
+            [&](float bx0, float by0, float bz0, float bx1, float by1, float bz1) {
+              return seg_box(bx0, by0, bz0, bx1, by1, bz1, o, inv, lo, hi, A.pad);
+            },
+            [&](bool v, uint32_t i) -> bool {
+              float t = v ? splat_t(L, i, o, d) : -1.0f;
+              const bool keep = t >= 0.0f && t >= lo && t < hi;
+              const uint32_t m = __ballot_sync(kFull, keep);
+              if (n + __popc(m) > kSplatCap) return false;
+              if (keep) {
+                const int p = n + __popc(m & lt);
+                buf->t[p] = t;
+                buf->id[p] = i;
+              }
+              n += __popc(m);
+              return true;
+            });
+        __syncwarp();
+        if (!ok) {
+          if (run > 1) {
+            run >>= 1;
+            continue;
+          }
+          // one slab with more samples than the buffer: its 15 smallest (t, index), one by one
+          const float tmin = lo, tmax = hi;
+          float pt = -__int_as_float(0x7f800000);
+          uint32_t pi = 0u;
+          bool first = true;
+          for (int taken = 0; taken < kKeep; ++taken) {
+            float bt = __int_as_float(0x7f800000);
+            uint32_t bi = 0xffffffffu;
+            warp_traverse_nodes(
+                L.s, L.s.nodes_ref, stk, buf->leaves, L.status,
+                [&](float bx0, float by0, float bz0, float bx1, float by1, float bz1) {
+                  return seg_box(bx0, by0, bz0, bx1, by1, bz1, o, inv, tmin, tmax, A.pad);
+                },
+                [&](bool v, uint32_t i) -> bool {
+                  float t = v ? splat_t(L, i, o, d) : -1.0f;
+                  if (t >= 0.0f && t >= tmin && t < tmax && (first || less_ti(pt, pi, t, i)) && less_ti(t, i, bt, bi)) {
+                    bt = t;
+                    bi = i;
+                  }
+                  return true;
+                });
+            for (int off = 16; off; off >>= 1) {
+              const float ot = __shfl_xor_sync(kFull, bt, off);
+              const uint32_t oi = __shfl_xor_sync(kFull, bi, off);
+              if (less_ti(ot, oi, bt, bi)) {
+                bt = ot;
+                bi = oi;
+              }
+            }
+            if (bi == 0xffffffffu) break;
+            res = over4(res, shade_sample(L, bi, bt, o, d, atten));
+            pt = bt;
+            pi = bi;
+            first = false;
+          }
+          k += 1;
+          continue;
+        }
+        if (n == 0) {
+          k = kend;
+          if (run < 4096) run <<= 1;
+          continue;
+        }
+        bitonic_sort(buf, n, lane);
+        // composite the slabs of the run
+        int cur = 0;
+        while (k < kend) {
+          const float tk = __ldg(A.slabs + k);
+          if (!(tk < texit) || res.w > 0.99f) break;
+          const float tmin = fmaxf(tenter, tk), tmax = fminf(texit, __ldg(A.slabs + k + 1));
+          // skip samples below this slab (beyond the 15 kept by an earlier slab)
+          for (;;) {
+            const int j = cur + (int)lane;
+            const uint32_t below = __ballot_sync(kFull, j < n && buf->t[j] < tmin);
+            const int c = __popc(below);
+            cur += c;
+            if (c < 32) break;
+          }
+          if (cur >= n) {
+            k = kend;
+            break;
+          }
+          const int j = cur + (int)lane;
+          const uint32_t inside = __ballot_sync(kFull, j < n && (int)lane < kKeep && buf->t[j] < tmax);
+          const int m = __popc(inside);
+          if (m == 0) {
+            // the next sample's slab: first slab whose end lies beyond it
+            const float tn = buf->t[cur];
+            k = max(k + 1, min(kend, first_above(A.slabs, k + 1, kend + 1, tn) - 1));
+            continue;
+          }
+          float4 col = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          if ((int)lane < m) col = shade_sample(L, buf->id[j], buf->t[j], o, d, atten);
+          for (int q = 0; q < m; ++q) {
+            const float4 c = make_float4(__shfl_sync(kFull, col.x, q), __shfl_sync(kFull, col.y, q),
+                                         __shfl_sync(kFull, col.z, q), __shfl_sync(kFull, col.w, q));
+            res = over4(res, c);
+          }
+          cur += m;
+          k += 1;
+        }
+        if (n < kSplatCap / 4 && run < 4096) run <<= 1;
+      }
+    }
+    res = over4(res, make_float4(0.0f, 0.0f, 0.0f, 1.0f));
+    if (lane == 0) L.image[(size_t)px + (size_t)L.width * (size_t)py] = res;
+  }
+}
+
+int splat_grid_blocks() {
+  static int cached = 0;
+  if (!cached) {
+    const size_t smem = sizeof(SplatBuf) * kSplatWarps;
+    cudaFuncSetAttribute(k_splat_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_splat_warp, kSplatWarps * 32, smem);
+    cached = sms * (per > 0 ? per : 1);
+  }
+  return cached;
+}
+
 }  // namespace
 
-cudaError_t launch_splat(const RenderLaunch& L, cudaStream_t st) {
+cudaError_t launch_splat(const RenderLaunch& L, cudaStream_t st, const float* slabs, int nslabs) {
   if (L.width <= 0 || L.height <= 0) return cudaSuccess;
   // An accepted sample point lies within the splat radius of its particle's centre, on the ray
   // segment being staged. The reference-bounds box holds the sphere of the bounds radius, so
@@ -252,9 +471,23 @@ cudaError_t launch_splat(const RenderLaunch& L, cudaStream_t st) {
   // the rounding of the sample point and of the box corners.
   const bool own_radius = (L.flags & kFlagSplatParticleRadius) != 0;
   float pad = (own_radius ? 0.0f : L.splat_rmax) + 4.0f * L.s.eps;
+  if (slabs && nslabs >= 2 && L.traversal != AARBF_TRAVERSAL_THREAD) {
+    SplatWarpArgs A;
+    A.slabs = slabs;
+    A.nslabs = nslabs;
+    A.pad = pad;
+    A.work_counter = L.work_counter;
+    A.warp_stacks = L.warp_stacks;
+    cudaError_t e = cudaMemsetAsync(L.work_counter, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    k_splat_warp<<<splat_grid_blocks(), kSplatWarps * 32, sizeof(SplatBuf) * kSplatWarps, st>>>(L, A);
+    return cudaGetLastError();
+  }
   dim3 grid((L.width + 15) / 16, (L.height + 7) / 8);
   k_splat<<<grid, kBlock, 0, st>>>(L, pad);
   return cudaGetLastError();
 }
+
+size_t splat_stack_words() { return (size_t)splat_grid_blocks() * kSplatWarps * kWarpStack; }
 
 }  // namespace aarbf

@@ -57,13 +57,15 @@ __device__ __forceinline__ void wctr(unsigned long long* c, int i, unsigned long
   if (c && (threadIdx.x & 31u) == 0) atomicAdd(c + i, v);
 }
 
-// Warp-wide traversal of the (traversal-bounds) BVH. box_test(child box) decides which children
-// to enter; on_particle(valid, i) is called by all lanes together for the particles of every
-// entered leaf (valid false on padding lanes) and returns false to abort. Returns false on abort
-// or stack overflow.
+// Warp-wide traversal of a BVH over the scene's topology: `nodes` is one of its node arrays
+// (traversal bounds s.nodes, reference bounds s.nodes_ref). box_test(child box) decides which
+// children to enter; on_particle(valid, i) is called by all lanes together for the particles of
+// every entered leaf (valid false on padding lanes) and returns false to abort. Returns false on
+// abort or stack overflow.
 template <class BoxTest, class OnParticle>
-__device__ bool warp_traverse(const SceneView& s, uint32_t* stk, uint32_t* leafbuf, uint32_t* status,
-                              BoxTest&& box_test, OnParticle&& on_particle, unsigned long long* ctr = nullptr) {
+__device__ bool warp_traverse_nodes(const SceneView& s, const Node* nodes, uint32_t* stk, uint32_t* leafbuf,
+                                    uint32_t* status, BoxTest&& box_test, OnParticle&& on_particle,
+                                    unsigned long long* ctr = nullptr) {
   const uint32_t lane = threadIdx.x & 31u, lt = lane_lt_mask();
   if (s.nleaves == 0) return true;
   const uint32_t ppl = s.ppl;
@@ -88,7 +90,7 @@ __device__ bool warp_traverse(const SceneView& s, uint32_t* stk, uint32_t* leafb
     bool h0 = false, h1 = false;
     uint2 ch = make_uint2(0u, 0u);
     if (valid) {
-      const Node* nd = s.nodes + node;
+      const Node* nd = nodes + node;
       float4 a = __ldg(&nd->a), b = __ldg(&nd->b), c = __ldg(&nd->c);
       ch = __ldg(reinterpret_cast<const uint2*>(&nd->d));
       h0 = box_test(a.x, a.y, a.z, a.w, b.x, b.y);
@@ -127,6 +129,14 @@ __device__ bool warp_traverse(const SceneView& s, uint32_t* stk, uint32_t* leafb
     __syncwarp();
   }
   return true;
+}
+
+// the traversal-bounds BVH (particles that can be hit)
+template <class BoxTest, class OnParticle>
+__device__ __forceinline__ bool warp_traverse(const SceneView& s, uint32_t* stk, uint32_t* leafbuf, uint32_t* status,
+                                              BoxTest&& box_test, OnParticle&& on_particle,
+                                              unsigned long long* ctr = nullptr) {
+  return warp_traverse_nodes(s, s.nodes, stk, leafbuf, status, box_test, on_particle, ctr);
 }
 
 }  // namespace aarbf

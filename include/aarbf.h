@@ -231,7 +231,9 @@ aarbf_status aarbf_render_diff_backward(aarbf_ctx *ctx, const aarbf_params *view
                                         int height, const float *grad_images, float *grad_xyz,
                                         float *grad_radius, float *grad_attr, float *grad_tf, void *stream);
 
-/* ParticleSplatRayGen (deviceCodeSplat.hlsl:58-193); writes image only. */
+/* ParticleSplatRayGen (deviceCodeSplat.hlsl:58-193); writes image only. One warp per pixel
+ * (AARBF_TRAVERSAL_AUTO; the first call with a new `unit` uploads a table of slab starts and
+ * synchronises `stream` once) or one thread per pixel (AARBF_TRAVERSAL_THREAD); identical bits. */
 aarbf_status aarbf_render_splat(aarbf_ctx *ctx, const aarbf_params *p, int width, int height,
                                 float *image, void *stream);
 /* CompositeGui TAA resolve (deviceCodeCommon.hlsl:67-115). Writes taa unless disable; bgra

@@ -274,8 +274,9 @@ def test_kernel_timing(ctx, orc, aarbf_mod):
     assert_bitexact(gi2, gi, "image (second timed render)")
 
 
+@pytest.mark.parametrize("traversal", [0, 2])  # one warp per pixel / one thread per pixel
 @pytest.mark.parametrize("native", [False, True])
-def test_splat_parity(ctx, orc, aarbf_mod, native):
+def test_splat_parity(ctx, orc, aarbf_mod, native, traversal):
     w, h = 32, 24
     if native:
         from aarbf import scenes
@@ -290,10 +291,42 @@ def test_splat_parity(ctx, orc, aarbf_mod, native):
         rp, r = reference_params(aarbf_mod, dom, w, h)
         rp.unit = float(np.float32(r * 0.5))
         scene, *_ = setup_both(ctx, orc, aarbf_mod, xyzw, None, 1, r)
+    rp.traversal = traversal
     _, gi = gpu_render(ctx, rp, w, h, splat=True)
     oi = scene.render_splat(orc.params_from(rp), w, h)
     assert_radiance(gi, oi, "splat image")
     assert (oi[..., :3] > 0).mean() > 0.01  # the view is not empty
+
+
+def test_splat_crowded_slab(ctx, orc, aarbf_mod):
+    """thousands of samples in one slab (particles on a sphere around the camera): the warp
+    kernel's staging overflows even for a single slab and takes the 15 smallest (t, index) by
+    repeated minimum traversals"""
+    from aarbf import scenes
+    rng = np.random.default_rng(8)
+    n = 3000
+    cam = scenes.orbit_camera(distance=2.5)
+    c, o = np.asarray(cam[1], np.float64), np.asarray(cam[0], np.float64)
+    fwd = (c - o) / np.linalg.norm(c - o)
+    side = np.cross(fwd, [0.0, 1.0, 0.0])
+    side /= np.linalg.norm(side)
+    up = np.cross(side, fwd)
+    ang = rng.uniform(-0.004, 0.004, (n, 2))
+    dirs = fwd[None] + ang[:, :1] * side[None] + ang[:, 1:] * up[None]
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    pos = o[None] + 2.5 * dirs
+    xyzw = np.concatenate([pos, rng.uniform(0, 1, (n, 1))], 1).astype(np.float32)
+    radii = np.full(n, 0.05, np.float32)
+    dom = orc.domain([xyzw])
+    cm, rm, dm = scenes.tf_linear_ramp()
+    w, h = 8, 8
+    cam_narrow = (cam[0], cam[1], cam[2], 0.004)
+    rp = scenes.native_params(cam_narrow, w, h, 0.05, 0.001, 50.0, dom)
+    scene, *_ = setup_both(ctx, orc, aarbf_mod, xyzw, radii, 1, 0.05, tf32=(cm, rm, dm))
+    _, gi = gpu_render(ctx, rp, w, h, splat=True)
+    oi = scene.render_splat(orc.params_from(rp), w, h)
+    assert (oi[..., 3] > 0).all()
+    assert_radiance(gi, oi, "splat image")
 
 
 def test_taa_parity(ctx, orc):
