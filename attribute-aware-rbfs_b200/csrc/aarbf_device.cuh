@@ -45,6 +45,13 @@ struct __align__(16) Node {
   uint4 d;   // child0 code, child1 code, parent, unused
 };
 
+// Four-wide node derived from the binary tree: node n lists the children of n's children (a
+// child that is a leaf stays itself), i.e. two binary levels per traversal step. One 32-byte
+// slot per child: lo.xyz, hi.xyz, child code (bit 31 = leaf; 0xffffffff = empty slot).
+struct __align__(16) WideNode {
+  float4 s[8];  // slot k: s[2k] = (lo.x, lo.y, lo.z, hi.x), s[2k+1] = (hi.y, hi.z, code, 0)
+};
+
 // ------------------------------------------------------------------------------------------
 // deterministic math
 // ------------------------------------------------------------------------------------------

@@ -131,6 +131,13 @@ aarbf_status run_refit(aarbf_ctx* ctx, cudaStream_t st) {
                   ctx->nodes_ref.as<Node>(), ctx->leaf_parent.as<uint32_t>(), ctx->counters.as<uint32_t>(),
                   ctx->leaf_box.as<float>(), ctx->leaf_eff.as<float>(), ctx->root_box.as<float>(), st),
      "refit");
+  if (ctx->nleaves > 1) {
+    const size_t wb = sizeof(WideNode) * (size_t)(ctx->nleaves - 1);
+    CK(ctx->wide.reserve(wb), "alloc");
+    CK(ctx->wide_ref.reserve(wb), "alloc");
+    CK(launch_collapse4(ctx->nodes.as<Node>(), ctx->nleaves, ctx->wide.as<WideNode>(), st), "collapse");
+    CK(launch_collapse4(ctx->nodes_ref.as<Node>(), ctx->nleaves, ctx->wide_ref.as<WideNode>(), st), "collapse");
+  }
   if (ctx->nleaves) {
     CK(cudaMemcpyAsync(ctx->root_box_host, ctx->root_box.ptr, 6 * sizeof(float), cudaMemcpyDeviceToHost, st),
        "root box");
@@ -173,6 +180,8 @@ void fill_scene_view(const aarbf_ctx* ctx, const float* cam_pos, SceneView& s) {
   s.rgeom = ctx->rgeom.as<float>();
   s.nodes = ctx->nodes.as<Node>();
   s.nodes_ref = ctx->nodes_ref.as<Node>();
+  s.wide = ctx->wide.as<WideNode>();
+  s.wide_ref = ctx->wide_ref.as<WideNode>();
   s.tf_color = ctx->tf_color.as<float4>();
   s.tf_density = ctx->tf_density.as<float>();
   s.n = ctx->n;
@@ -333,7 +342,8 @@ aarbf_status aarbf_destroy(aarbf_ctx* ctx) {
                     &ctx->sorted_keys, &ctx->tf_color, &ctx->tf_radius, &ctx->tf_density, &ctx->noise,
                     &ctx->fb_accum, &ctx->fb_image, &ctx->status, &ctx->work, &ctx->samples,
                     &ctx->noise_buf, &ctx->warp_stacks, &ctx->diff_views, &ctx->diff_ckpt, &ctx->diff_grad,
-                    &ctx->posq, &ctx->colq, &ctx->origin, &ctx->reval, &ctx->splat_slabs};
+                    &ctx->posq, &ctx->colq, &ctx->origin, &ctx->reval, &ctx->splat_slabs, &ctx->wide,
+                    &ctx->wide_ref};
   for (DevBuf* b : bufs) b->release();
   for (auto* v : {&ctx->ev_pending, &ctx->ev_free})
     for (auto& ev : *v)

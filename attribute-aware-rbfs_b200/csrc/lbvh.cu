@@ -183,6 +183,43 @@ __global__ void k_refit(const float4* __restrict__ rec0, const float* __restrict
   }
 }
 
+// one thread per binary internal node: the 4-wide node of its grandchildren
+__global__ void k_collapse4(const Node* __restrict__ nodes, uint32_t ninternal, WideNode* __restrict__ wide) {
+  const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= ninternal) return;
+  float box[4][6];
+  uint32_t code[4];
+  int k = 0;
+  const Node nd = nodes[n];
+  const float* f = reinterpret_cast<const float*>(&nd);
+  const uint32_t ch[2] = {nd.d.x, nd.d.y};
+  for (int c = 0; c < 2; ++c) {
+    if (ch[c] & kLeafBit) {
+      for (int q = 0; q < 6; ++q) box[k][q] = f[6 * c + q];
+      code[k++] = ch[c];
+    } else {
+      const Node g = nodes[ch[c]];
+      const float* gf = reinterpret_cast<const float*>(&g);
+      const uint32_t gc[2] = {g.d.x, g.d.y};
+      for (int e = 0; e < 2; ++e) {
+        for (int q = 0; q < 6; ++q) box[k][q] = gf[6 * e + q];
+        code[k++] = gc[e];
+      }
+    }
+  }
+  WideNode w;
+  for (int j = 0; j < 4; ++j) {
+    if (j < k) {
+      w.s[2 * j] = make_float4(box[j][0], box[j][1], box[j][2], box[j][3]);
+      w.s[2 * j + 1] = make_float4(box[j][4], box[j][5], __uint_as_float(code[j]), 0.0f);
+    } else {
+      w.s[2 * j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      w.s[2 * j + 1] = make_float4(0.0f, 0.0f, __uint_as_float(0xffffffffu), 0.0f);
+    }
+  }
+  wide[n] = w;
+}
+
 }  // namespace
 
 cudaError_t launch_prepass(const float4* xyzw, const float* radii, uint64_t n, const float4* tf_color, int nc,
@@ -191,6 +228,13 @@ cudaError_t launch_prepass(const float4* xyzw, const float* radii, uint64_t n, c
   if (!n) return cudaSuccess;
   k_prepass<<<blocks_for(n, 256), 256, 0, st>>>(xyzw, radii, n, tf_color, nc, tf_radius, nr, rbf_radius,
                                                 alpha_floor, rec0, w4, rgeom);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_collapse4(const Node* nodes, uint32_t nleaves, WideNode* wide, cudaStream_t st) {
+  if (nleaves < 2) return cudaSuccess;
+  const uint32_t ni = nleaves - 1;
+  k_collapse4<<<(ni + 255) / 256, 256, 0, st>>>(nodes, ni, wide);
   return cudaGetLastError();
 }
 

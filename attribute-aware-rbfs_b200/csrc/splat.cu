@@ -333,8 +333,8 @@ __global__ void __launch_bounds__(kSplatWarps * 32) k_splat_warp(const __grid_co
         const int kend = min(k + run, A.nslabs - 1);
         const float lo = fmaxf(tenter, ts), hi = fminf(texit, __ldg(A.slabs + kend));
         int n = 0;
-        const bool ok = warp_traverse_nodes(
-            L.s, L.s.nodes_ref, stk, buf->leaves, L.status,
+        const bool ok = warp_traverse_wide(
+            L.s, L.s.wide_ref, stk, buf->leaves, L.status,
             [&](float bx0, float by0, float bz0, float bx1, float by1, float bz1) {
               return seg_box(bx0, by0, bz0, bx1, by1, bz1, o, inv, lo, hi, A.pad);
             },
@@ -365,8 +365,8 @@ __global__ void __launch_bounds__(kSplatWarps * 32) k_splat_warp(const __grid_co
           for (int taken = 0; taken < kKeep; ++taken) {
             float bt = __int_as_float(0x7f800000);
             uint32_t bi = 0xffffffffu;
-            warp_traverse_nodes(
-                L.s, L.s.nodes_ref, stk, buf->leaves, L.status,
+            warp_traverse_wide(
+                L.s, L.s.wide_ref, stk, buf->leaves, L.status,
                 [&](float bx0, float by0, float bz0, float bx1, float by1, float bz1) {
                   return seg_box(bx0, by0, bz0, bx1, by1, bz1, o, inv, tmin, tmax, A.pad);
                 },

@@ -57,15 +57,16 @@ __device__ __forceinline__ void wctr(unsigned long long* c, int i, unsigned long
   if (c && (threadIdx.x & 31u) == 0) atomicAdd(c + i, v);
 }
 
-// Warp-wide traversal of a BVH over the scene's topology: `nodes` is one of its node arrays
-// (traversal bounds s.nodes, reference bounds s.nodes_ref). box_test(child box) decides which
-// children to enter; on_particle(valid, i) is called by all lanes together for the particles of
-// every entered leaf (valid false on padding lanes) and returns false to abort. Returns false on
-// abort or stack overflow.
+// Warp-wide traversal of a BVH in its four-wide form (WideNode: two binary levels per node).
+// Each step takes up to 8 nodes from the warp's stack; lane 4j + k tests child k of node j with
+// box_test(child box) and pushes the inner children it enters (ballot-compacted);
+// on_particle(valid, i) is then called by all lanes together for the particles of every entered
+// leaf (valid false on padding lanes) and returns false to abort. Returns false on abort or
+// stack overflow.
 template <class BoxTest, class OnParticle>
-__device__ bool warp_traverse_nodes(const SceneView& s, const Node* nodes, uint32_t* stk, uint32_t* leafbuf,
-                                    uint32_t* status, BoxTest&& box_test, OnParticle&& on_particle,
-                                    unsigned long long* ctr = nullptr) {
+__device__ bool warp_traverse_wide(const SceneView& s, const WideNode* wide, uint32_t* stk, uint32_t* leafbuf,
+                                   uint32_t* status, BoxTest&& box_test, OnParticle&& on_particle,
+                                   unsigned long long* ctr = nullptr) {
   const uint32_t lane = threadIdx.x & 31u, lt = lane_lt_mask();
   if (s.nleaves == 0) return true;
   const uint32_t ppl = s.ppl;
@@ -81,36 +82,33 @@ __device__ bool warp_traverse_nodes(const SceneView& s, const Node* nodes, uint3
   int sp = 1;
   __syncwarp();
   for (int guard = 0; sp > 0 && guard < (1 << 24); ++guard) {
-    const int take = sp < 32 ? sp : 32;
+    const int take = sp < 8 ? sp : 8;
     const int base = sp - take;
-    const bool valid = (int)lane < take;
-    uint32_t node = valid ? stk[base + lane] : 0u;
+    const int slot = (int)(lane >> 2);
+    const bool valid = slot < take;
+    const uint32_t node = valid ? stk[base + slot] : 0u;
     __syncwarp();
     sp = base;
-    bool h0 = false, h1 = false;
-    uint2 ch = make_uint2(0u, 0u);
+    bool hit = false;
+    uint32_t code = 0xffffffffu;
     if (valid) {
-      const Node* nd = nodes + node;
-      float4 a = __ldg(&nd->a), b = __ldg(&nd->b), c = __ldg(&nd->c);
-      ch = __ldg(reinterpret_cast<const uint2*>(&nd->d));
-      h0 = box_test(a.x, a.y, a.z, a.w, b.x, b.y);
-      h1 = box_test(b.z, b.w, c.x, c.y, c.z, c.w);
+      const float4* p = wide[node].s + 2 * (lane & 3u);
+      const float4 a = __ldg(p), b = __ldg(p + 1);
+      code = __float_as_uint(b.z);
+      hit = code != 0xffffffffu && box_test(a.x, a.y, a.z, a.w, b.x, b.y);
     }
-    const bool i0 = h0 && !(ch.x & kLeafBit), i1 = h1 && !(ch.y & kLeafBit);
-    const bool l0 = h0 && (ch.x & kLeafBit), l1 = h1 && (ch.y & kLeafBit);
-    const uint32_t m0 = __ballot_sync(kFull, i0), m1 = __ballot_sync(kFull, i1);
-    const int n0 = __popc(m0), n1 = __popc(m1);
-    if (sp + n0 + n1 > kWarpStack) {
+    const bool inner = hit && !(code & kLeafBit), leaf = hit && (code & kLeafBit);
+    const uint32_t m = __ballot_sync(kFull, inner);
+    const int ni = __popc(m);
+    if (sp + ni > kWarpStack) {
       if (lane == 0) atomicOr(status, kStatusStackOverflow);
       return false;
     }
-    if (i0) stk[sp + __popc(m0 & lt)] = ch.x;
-    if (i1) stk[sp + n0 + __popc(m1 & lt)] = ch.y;
-    sp += n0 + n1;
-    const uint32_t q0 = __ballot_sync(kFull, l0), q1 = __ballot_sync(kFull, l1);
-    const int c0 = __popc(q0), nl = c0 + __popc(q1);
-    if (l0) leafbuf[__popc(q0 & lt)] = ch.x & ~kLeafBit;
-    if (l1) leafbuf[c0 + __popc(q1 & lt)] = ch.y & ~kLeafBit;
+    if (inner) stk[sp + __popc(m & lt)] = code;
+    sp += ni;
+    const uint32_t q = __ballot_sync(kFull, leaf);
+    const int nl = __popc(q);
+    if (leaf) leafbuf[__popc(q & lt)] = code & ~kLeafBit;
     __syncwarp();
     const uint32_t total = (uint32_t)nl * ppl;
     wctr(ctr, kWcIters, 1);
@@ -120,8 +118,8 @@ __device__ bool warp_traverse_nodes(const SceneView& s, const Node* nodes, uint3
       bool v = j < total;
       uint64_t i = 0;
       if (v) {
-        uint32_t leaf = leafbuf[j / ppl];
-        i = (uint64_t)leaf * ppl + (j % ppl);
+        uint32_t lf = leafbuf[j / ppl];
+        i = (uint64_t)lf * ppl + (j % ppl);
         v = i < s.n;
       }
       if (!on_particle(v, (uint32_t)i)) return false;
@@ -136,7 +134,7 @@ template <class BoxTest, class OnParticle>
 __device__ __forceinline__ bool warp_traverse(const SceneView& s, uint32_t* stk, uint32_t* leafbuf, uint32_t* status,
                                               BoxTest&& box_test, OnParticle&& on_particle,
                                               unsigned long long* ctr = nullptr) {
-  return warp_traverse_nodes(s, s.nodes, stk, leafbuf, status, box_test, on_particle, ctr);
+  return warp_traverse_wide(s, s.wide, stk, leafbuf, status, box_test, on_particle, ctr);
 }
 
 }  // namespace aarbf
