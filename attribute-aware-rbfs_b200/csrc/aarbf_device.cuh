@@ -45,11 +45,17 @@ struct __align__(16) Node {
   uint4 d;   // child0 code, child1 code, parent, unused
 };
 
-// Four-wide node derived from the binary tree: node n lists the children of n's children (a
-// child that is a leaf stays itself), i.e. two binary levels per traversal step. One 32-byte
-// slot per child: lo.xyz, hi.xyz, child code (bit 31 = leaf; 0xffffffff = empty slot).
+// Wide node derived from the binary tree: node n lists up to kBvhWidth descendants of binary
+// node n that together cover its subtree (its children, with the inner ones of largest surface
+// area replaced by their own children until the node is full), so one traversal step descends
+// several binary levels. One 32-byte slot per child: lo.xyz, hi.xyz, child code (bit 31 = leaf;
+// 0xffffffff = empty slot). Every binary inner node has its wide node (the same index).
+#ifndef AARBF_BVH_WIDTH
+#define AARBF_BVH_WIDTH 4
+#endif
+constexpr int kBvhWidth = AARBF_BVH_WIDTH;
 struct __align__(16) WideNode {
-  float4 s[8];  // slot k: s[2k] = (lo.x, lo.y, lo.z, hi.x), s[2k+1] = (hi.y, hi.z, code, 0)
+  float4 s[2 * kBvhWidth];  // slot k: s[2k] = (lo.x, lo.y, lo.z, hi.x), s[2k+1] = (hi.y, hi.z, code, 0)
 };
 
 // ------------------------------------------------------------------------------------------

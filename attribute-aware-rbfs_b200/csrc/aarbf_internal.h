@@ -44,8 +44,8 @@ struct SceneView {
   const float* rgeom;  // bounds radius, -1 = skipped by the bounds program
   const Node* nodes;      // traversal bounds (particles that can be hit)
   const Node* nodes_ref;  // reference bounds (splatting)
-  const WideNode* wide;      // four-wide form of nodes (what the warp traversals read)
-  const WideNode* wide_ref;  // four-wide form of nodes_ref
+  const WideNode* wide;      // wide form of nodes (what the warp traversals read)
+  const WideNode* wide_ref;  // wide form of nodes_ref
   const float4* tf_color;
   const float* tf_density;
   uint64_t n;
@@ -111,8 +111,10 @@ cudaError_t launch_prepass(const float4* xyzw, const float* radii, uint64_t n, c
                            float4* rec0, float4* w4, float* rgeom, cudaStream_t st);
 cudaError_t launch_karras(const uint64_t* sorted_keys, uint64_t n, uint32_t ppl, uint32_t nleaves,
                           Node* nodes, Node* nodes_ref, uint32_t* leaf_parent, cudaStream_t st);
-// four-wide nodes (two binary levels per node) of the binary tree; nleaves - 1 of them
-cudaError_t launch_collapse4(const Node* nodes, uint32_t nleaves, WideNode* wide, cudaStream_t st);
+// largest bounds radius of the scene into *out (device)
+cudaError_t launch_max_radius(const float* rgeom, uint64_t n, float* out, cudaStream_t st);
+// wide nodes (several binary levels per node) of the binary tree; nleaves - 1 of them
+cudaError_t launch_collapse(const Node* nodes, uint32_t nleaves, WideNode* wide, cudaStream_t st);
 cudaError_t launch_refit(const float4* rec0, const float* rgeom, uint64_t n, uint32_t ppl,
                          uint32_t nleaves, Node* nodes, Node* nodes_ref, const uint32_t* leaf_parent,
                          uint32_t* counters, float* leaf_box, float* leaf_eff, float* root_box,
@@ -228,7 +230,7 @@ struct aarbf_ctx {
   // status word, persistent-kernel work counter, per-sample colour planes
   aarbf::DevBuf status, work, samples, noise_buf, warp_stacks;
   float max_radius = 0.0f;
-  aarbf::DevBuf wide, wide_ref;  // four-wide forms of nodes / nodes_ref
+  aarbf::DevBuf wide, wide_ref;  // wide forms of nodes / nodes_ref
   aarbf::DevBuf splat_slabs;      // slab starts of the splat kernel, for splat_spacing
   float splat_spacing = 0.0f;
   int splat_nslabs = 0;

@@ -135,20 +135,17 @@ aarbf_status run_refit(aarbf_ctx* ctx, cudaStream_t st) {
     const size_t wb = sizeof(WideNode) * (size_t)(ctx->nleaves - 1);
     CK(ctx->wide.reserve(wb), "alloc");
     CK(ctx->wide_ref.reserve(wb), "alloc");
-    CK(launch_collapse4(ctx->nodes.as<Node>(), ctx->nleaves, ctx->wide.as<WideNode>(), st), "collapse");
-    CK(launch_collapse4(ctx->nodes_ref.as<Node>(), ctx->nleaves, ctx->wide_ref.as<WideNode>(), st), "collapse");
+    CK(launch_collapse(ctx->nodes.as<Node>(), ctx->nleaves, ctx->wide.as<WideNode>(), st), "collapse");
+    CK(launch_collapse(ctx->nodes_ref.as<Node>(), ctx->nleaves, ctx->wide_ref.as<WideNode>(), st), "collapse");
   }
-  if (ctx->nleaves) {
-    CK(cudaMemcpyAsync(ctx->root_box_host, ctx->root_box.ptr, 6 * sizeof(float), cudaMemcpyDeviceToHost, st),
-       "root box");
-  }
-  // largest bounds radius (host side; one pass over n floats)
-  std::vector<float> rg(n);
-  if (n) CK(cudaMemcpyAsync(rg.data(), ctx->rgeom.ptr, n * sizeof(float), cudaMemcpyDeviceToHost, st), "radii");
+  // root box (6 floats) and the largest bounds radius (slot 6), read back in one copy
+  float* rb = ctx->root_box.as<float>();
+  CK(launch_max_radius(ctx->rgeom.as<float>(), n, rb + 6, st), "max radius");
+  float host[7] = {0, 0, 0, 0, 0, 0, 0};
+  CK(cudaMemcpyAsync(host, rb, sizeof(host), cudaMemcpyDeviceToHost, st), "root box");
   CK(cudaStreamSynchronize(st), "refit sync");
-  float mx = 0.0f;
-  for (float r : rg) mx = std::fmax(mx, r);
-  ctx->max_radius = mx;
+  if (ctx->nleaves) memcpy(ctx->root_box_host, host, 6 * sizeof(float));
+  ctx->max_radius = host[6];
   ctx->built = true;
   return AARBF_OK;
 }

@@ -183,32 +183,51 @@ __global__ void k_refit(const float4* __restrict__ rec0, const float* __restrict
   }
 }
 
-// one thread per binary internal node: the 4-wide node of its grandchildren
-__global__ void k_collapse4(const Node* __restrict__ nodes, uint32_t ninternal, WideNode* __restrict__ wide) {
+// largest non-negative bounds radius (max over the float bits, which order like the values)
+__global__ void k_max_radius(const float* __restrict__ rgeom, uint64_t n, int* __restrict__ out) {
+  float m = 0.0f;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    m = fmaxf(m, __ldg(rgeom + i));
+  for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMax(out, __float_as_int(m));
+}
+
+// one thread per binary inner node: its wide node
+__global__ void k_collapse(const Node* __restrict__ nodes, uint32_t ninternal, WideNode* __restrict__ wide) {
   const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= ninternal) return;
-  float box[4][6];
-  uint32_t code[4];
+  constexpr int W = kBvhWidth;
+  float box[W][6];
+  uint32_t code[W];
   int k = 0;
-  const Node nd = nodes[n];
-  const float* f = reinterpret_cast<const float*>(&nd);
-  const uint32_t ch[2] = {nd.d.x, nd.d.y};
-  for (int c = 0; c < 2; ++c) {
-    if (ch[c] & kLeafBit) {
-      for (int q = 0; q < 6; ++q) box[k][q] = f[6 * c + q];
-      code[k++] = ch[c];
-    } else {
-      const Node g = nodes[ch[c]];
-      const float* gf = reinterpret_cast<const float*>(&g);
-      const uint32_t gc[2] = {g.d.x, g.d.y};
-      for (int e = 0; e < 2; ++e) {
-        for (int q = 0; q < 6; ++q) box[k][q] = gf[6 * e + q];
-        code[k++] = gc[e];
+  auto take = [&](const Node& nd, int c, int at) {
+    const float* f = reinterpret_cast<const float*>(&nd);
+    for (int q = 0; q < 6; ++q) box[at][q] = f[6 * c + q];
+    code[at] = c == 0 ? nd.d.x : nd.d.y;
+  };
+  const Node root = nodes[n];
+  take(root, 0, k++);
+  take(root, 1, k++);
+  // open the inner entry of largest surface area until the node is full
+  while (k < W) {
+    int best = -1;
+    float barea = -1.0f;
+    for (int j = 0; j < k; ++j) {
+      if (code[j] & kLeafBit) continue;
+      const float dx = box[j][3] - box[j][0], dy = box[j][4] - box[j][1], dz = box[j][5] - box[j][2];
+      const float area = (dx * dy + dy * dz) + dz * dx;
+      if (area > barea) {  // empty (NaN) subtrees are never opened
+        barea = area;
+        best = j;
       }
     }
+    if (best < 0) break;
+    const Node g = nodes[code[best]];
+    take(g, 0, best);
+    take(g, 1, k++);
   }
   WideNode w;
-  for (int j = 0; j < 4; ++j) {
+  for (int j = 0; j < W; ++j) {
     if (j < k) {
       w.s[2 * j] = make_float4(box[j][0], box[j][1], box[j][2], box[j][3]);
       w.s[2 * j + 1] = make_float4(box[j][4], box[j][5], __uint_as_float(code[j]), 0.0f);
@@ -231,10 +250,19 @@ cudaError_t launch_prepass(const float4* xyzw, const float* radii, uint64_t n, c
   return cudaGetLastError();
 }
 
-cudaError_t launch_collapse4(const Node* nodes, uint32_t nleaves, WideNode* wide, cudaStream_t st) {
+cudaError_t launch_max_radius(const float* rgeom, uint64_t n, float* out, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float), st);
+  if (e != cudaSuccess || !n) return e;
+  int blocks = (int)((n + 255) / 256);
+  if (blocks > 4096) blocks = 4096;
+  k_max_radius<<<blocks, 256, 0, st>>>(rgeom, n, reinterpret_cast<int*>(out));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_collapse(const Node* nodes, uint32_t nleaves, WideNode* wide, cudaStream_t st) {
   if (nleaves < 2) return cudaSuccess;
   const uint32_t ni = nleaves - 1;
-  k_collapse4<<<(ni + 255) / 256, 256, 0, st>>>(nodes, ni, wide);
+  k_collapse<<<(ni + 255) / 256, 256, 0, st>>>(nodes, ni, wide);
   return cudaGetLastError();
 }
 

@@ -57,8 +57,9 @@ __device__ __forceinline__ void wctr(unsigned long long* c, int i, unsigned long
   if (c && (threadIdx.x & 31u) == 0) atomicAdd(c + i, v);
 }
 
-// Warp-wide traversal of a BVH in its four-wide form (WideNode: two binary levels per node).
-// Each step takes up to 8 nodes from the warp's stack; lane 4j + k tests child k of node j with
+// Warp-wide traversal of a BVH in its wide form (WideNode: kBvhWidth children per node). Each
+// step takes up to 32 / kBvhWidth nodes from the warp's stack; lane kBvhWidth j + k tests child k
+// of node j with
 // box_test(child box) and pushes the inner children it enters (ballot-compacted);
 // on_particle(valid, i) is then called by all lanes together for the particles of every entered
 // leaf (valid false on padding lanes) and returns false to abort. Returns false on abort or
@@ -82,9 +83,10 @@ __device__ bool warp_traverse_wide(const SceneView& s, const WideNode* wide, uin
   int sp = 1;
   __syncwarp();
   for (int guard = 0; sp > 0 && guard < (1 << 24); ++guard) {
-    const int take = sp < 8 ? sp : 8;
+    constexpr int kPer = 32 / kBvhWidth;
+    const int take = sp < kPer ? sp : kPer;
     const int base = sp - take;
-    const int slot = (int)(lane >> 2);
+    const int slot = (int)lane / kBvhWidth;
     const bool valid = slot < take;
     const uint32_t node = valid ? stk[base + slot] : 0u;
     __syncwarp();
@@ -92,7 +94,7 @@ __device__ bool warp_traverse_wide(const SceneView& s, const WideNode* wide, uin
     bool hit = false;
     uint32_t code = 0xffffffffu;
     if (valid) {
-      const float4* p = wide[node].s + 2 * (lane & 3u);
+      const float4* p = wide[node].s + 2 * ((int)lane % kBvhWidth);
       const float4 a = __ldg(p), b = __ldg(p + 1);
       code = __float_as_uint(b.z);
       hit = code != 0xffffffffu && box_test(a.x, a.y, a.z, a.w, b.x, b.y);
