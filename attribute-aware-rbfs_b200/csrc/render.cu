@@ -1198,6 +1198,172 @@ void track_majorant_warp(const RenderLaunch& L, Tracker& tr_io, const Ray& ray_i
   tr_io = tr;
 }
 
+// stochasticMarching (deviceCodeRBF.hlsl:67-139) with the warp: the steps of a chunk (up to 32)
+// are evaluated one per lane against the particles staged for the chunk's segment; the step
+// positions are the reference's running sum t += unit and the accumulated density / shadow
+// opacity and the stopping test run in step order (all lanes, values by shuffle), so every float
+// matches the sequential tracker. A chunk whose candidates overflow the buffer is halved; a single
+// step that still overflows is evaluated by a direct warp traversal.
+template <int CAPW>
+__device__ bool stage_segment(const SceneView& s, const Ray& ray, float3 inv, float ta, float tb, WarpBuf<CAPW>* buf,
+                              uint32_t* stk, uint32_t* status, int& n) {
+  const uint32_t lt = lane_lt_mask();
+  const float eps = s.eps;
+  n = 0;
+  const bool ok = warp_traverse(
+      s, stk, buf->leaves, status,
+      [&](float lx, float ly, float lz, float hx, float hy, float hz) {
+        return seg_box(lx, ly, lz, hx, hy, hz, ray.o, inv, ta, tb, eps);
+      },
+      [&](bool v, uint32_t i) -> bool {
+        bool keep = false;
+        float a = 0.0f, b = 0.0f;
+        if (v) {
+          float4 r = part_rec(s, i);
+          if (r.w > 0.0f) {
+            float vx = r.x - ray.o.x, vy = r.y - ray.o.y, vz = r.z - ray.o.z;
+            float tc = (vx * ray.d.x + vy * ray.d.y) + vz * ray.d.z;
+            float wx = vx - tc * ray.d.x, wy = vy - tc * ray.d.y, wz = vz - tc * ray.d.z;
+            float h2 = (wx * wx + wy * wy) + wz * wz;
+            float R = r.w * (1.0f + 0x1p-10f) + eps;
+            if (!(h2 > R * R)) {
+              float half = sqrtf(R * R - h2) + eps;
+              a = tc - half;
+              b = tc + half;
+              keep = !(b < ta || a > tb);
+            }
+          }
+        }
+        const uint32_t m = __ballot_sync(kFull, keep);
+        const int cnt = __popc(m);
+        if (n + cnt > CAPW) return false;
+        if (keep) {
+          int p = n + __popc(m & lt);
+          buf->idx[p] = i;
+          buf->lo[p] = a;
+          buf->hi[p] = b;
+        }
+        n += cnt;
+        return true;
+      });
+  __syncwarp();
+  return ok;
+}
+
+template <int CAPW>
+__device__ __forceinline__ void track_march_warp_body(const RenderLaunch& L, Tracker& tr, const Ray& ray,
+                                                      WarpBuf<CAPW>* buf, uint32_t* stk) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const SceneView& s = L.s;
+  const float rhs = -dlog(1.0f - tr.random * 0.99f);
+  const float3 inv = make_float3(1.0f / ray.d.x, 1.0f / ray.d.y, 1.0f / ray.d.z);
+  int m = 32;
+  for (int guard = 0; guard < (1 << 22); ++guard) {
+    if (tr.i >= kMaxDepth) return;
+    // the chunk's step positions: the running sum, lane j keeps step j
+    float tj = 0.0f, t = tr.t;
+    for (int j = 0; j < m; ++j) {
+      t = t + L.unit;
+      if ((int)lane == j) tj = t;
+    }
+    const float tfirst = __shfl_sync(kFull, tj, 0);
+    if (!(tfirst < ray.tmax)) {
+      tr.t = tfirst;
+      return;
+    }
+    const float tb = fminf(t, ray.tmax);
+    int n = 0;
+    bool direct = false;
+    if (!stage_segment<CAPW>(s, ray, inv, tfirst, tb, buf, stk, L.status, n)) {
+      if (m > 1) {
+        m >>= 1;
+        continue;
+      }
+      direct = true;
+    }
+    const bool active = (int)lane < m;
+    const float3 x = make_float3(ray.o.x + tj * ray.d.x, ray.o.y + tj * ray.d.y, ray.o.z + tj * ray.d.z);
+    Sample smp;
+    sample_clear(smp);
+    if (!direct) {
+      for (int c = 0; c < n; ++c) {
+        const bool in = active && tj < ray.tmax && tj >= buf->lo[c] && tj <= buf->hi[c];
+        if (in) eval_particle(s, buf->idx[c], x, smp);
+      }
+    } else {
+      const float3 x0 = make_float3(__shfl_sync(kFull, x.x, 0), __shfl_sync(kFull, x.y, 0), __shfl_sync(kFull, x.z, 0));
+      Sample d0 = warp_point<CAPW>(s, x0, buf, stk, L.status, L.counters);
+      if (lane == 0) smp = d0;
+    }
+    const float D = (float)smp.a0 * kFixInv;
+    const bool ne = active && smp.count > 0 && D > 0.0f;
+    const float dens = ne ? sample_density(L, D) : 0.0f;
+    const float op = (ne && tr.shadow) ? (1.0f - dexp(-dens)) : 0.0f;
+    // the sequential tracker over the chunk's steps
+    int stop = -1;
+    float lhs = tr.lhs, alpha = tr.albedo.w;
+    for (int j = 0; j < m; ++j) {
+      if (tr.i + j >= kMaxDepth) {  // the step budget runs out before step j
+        tr.i = kMaxDepth;
+        tr.t = j ? __shfl_sync(kFull, tj, j - 1) : tr.t;
+        tr.lhs = lhs;
+        tr.albedo.w = alpha;
+        return;
+      }
+      const float tjj = __shfl_sync(kFull, tj, j);
+      if (tjj >= ray.tmax) {
+        tr.t = tjj;
+        tr.i += j;
+        tr.lhs = lhs;
+        tr.albedo.w = alpha;
+        return;
+      }
+      if (!__shfl_sync(kFull, ne, j)) continue;
+      lhs = lhs + __shfl_sync(kFull, dens, j);
+      if (lhs > rhs && !tr.shadow) {
+        stop = j;
+        break;
+      }
+      if (tr.shadow) {
+        alpha = alpha + __shfl_sync(kFull, op, j);
+        if (alpha >= 1.0f) {
+          alpha = 1.0f;
+          stop = j;
+          break;
+        }
+      }
+    }
+    if (stop >= 0) {
+      tr.t = __shfl_sync(kFull, tj, stop);
+      tr.i += stop;
+      tr.lhs = lhs;
+      if (tr.shadow) {
+        tr.albedo.w = alpha;
+      } else {
+        float3 c = make_float3(0.0f, 0.0f, 0.0f);
+        if ((int)lane == stop) c = sample_color(L, smp, D);
+        tr.albedo = make_float4(__shfl_sync(kFull, c.x, stop), __shfl_sync(kFull, c.y, stop),
+                                __shfl_sync(kFull, c.z, stop), 1.0f);
+      }
+      return;
+    }
+    tr.t = t;
+    tr.i += m;
+    tr.lhs = lhs;
+    tr.albedo.w = alpha;
+    if (m < 32) m <<= 1;
+  }
+}
+
+template <int CAPW>
+__device__ __noinline__ void track_march_warp(const RenderLaunch& L, Tracker& tr_io, const Ray& ray_io,
+                                              WarpBuf<CAPW>* buf, uint32_t* stk) {
+  Tracker tr = tr_io;
+  const Ray ray = ray_io;
+  track_march_warp_body<CAPW>(L, tr, ray, buf, stk);
+  tr_io = tr;
+}
+
 // persistent warps; an item is one sample of one pixel, ordered as in k_render
 // items of one render: one sample of one pixel, 32 consecutive items = one sample of an 8x4 tile
 __device__ __forceinline__ uint32_t warp_items(const RenderLaunch& L) {
@@ -1206,8 +1372,10 @@ __device__ __forceinline__ uint32_t warp_items(const RenderLaunch& L) {
   return tiles_x * ((uint32_t)(L.height + 3) / 4u) * 32u * spp;
 }
 
-// one work item of the ray-per-warp kernel (all lanes of the warp)
-template <int CAPW>
+// one work item of the ray-per-warp kernel (all lanes of the warp); MARCH: stochastic marching
+// (blue-noise mode), else delta tracking with per-bin majorants, each in its own kernel so neither
+// carries the other's code
+template <int CAPW, bool MARCH>
 __device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t item, WarpBuf<CAPW>* buf,
                                                  uint32_t* stk) {
   const uint32_t lane = threadIdx.x & 31u;
@@ -1224,7 +1392,10 @@ __device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t
   const long long c0 = cost ? clock64() : 0;
   float noise = 0.0f;
   float4 c = raygen_generic(L, (L.frame_id + k) & 0xffffu, px, py, noise, lane == 0,
-                            [&](Tracker& tr, const Ray& r, bool) { track_majorant_warp<CAPW>(L, tr, r, buf, stk); });
+                            [&](Tracker& tr, const Ray& r, bool) {
+                              if (MARCH) track_march_warp<CAPW>(L, tr, r, buf, stk);
+                              else track_majorant_warp<CAPW>(L, tr, r, buf, stk);
+                            });
   if (cost) c.w = (float)(clock64() - c0);
   if (lane == 0) {
     L.samples[(size_t)k * plane + ofs] = c;
@@ -1232,7 +1403,7 @@ __device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t
   }
 }
 
-template <int CAPW>
+template <int CAPW, bool MARCH>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks) k_render_warp(const __grid_constant__ RenderLaunch L) {
   extern __shared__ __align__(16) char smem[];
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
@@ -1244,7 +1415,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks) k_render_
     if (lane == 0) item = atomicAdd(L.work_counter, 1u);
     item = __shfl_sync(kFull, item, 0);
     if (item >= total) break;
-    render_warp_item<CAPW>(L, item, buf, stk);
+    render_warp_item<CAPW, MARCH>(L, item, buf, stk);
   }
 }
 
@@ -1270,7 +1441,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks)
       if (item_ofs[mid] <= item) lo = mid;
       else hi = mid;
     }
-    render_warp_item<CAPW>(Ls[lo], (uint32_t)(item - item_ofs[lo]), buf, stk);
+    render_warp_item<CAPW, false>(Ls[lo], (uint32_t)(item - item_ofs[lo]), buf, stk);
   }
 }
 
@@ -1400,12 +1571,17 @@ cudaError_t warp_grid(int* blocks) {
   if (!cached) {
     const size_t smem = sizeof(WarpBuf<CAPW>) * kWarpsPerBlock;
     cudaError_t e =
-        cudaFuncSetAttribute(k_render_warp<CAPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_render_warp<CAPW, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_render_warp<CAPW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    int dev = 0, sms = 0, per_sm = 0;
+    int dev = 0, sms = 0, per_sm = 0, per_m = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_warp<CAPW>, kWarpsPerBlock * 32, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_warp<CAPW, false>, kWarpsPerBlock * 32, smem);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_m, k_render_warp<CAPW, true>, kWarpsPerBlock * 32, smem);
+    per_sm = per_m > per_sm ? per_m : per_sm;
     if (e != cudaSuccess) return e;
     cached = sms * (per_sm > 0 ? per_sm : 1);
   }
@@ -1421,7 +1597,10 @@ cudaError_t launch_warp(const RenderLaunch& L, cudaStream_t st, const cudaEvent_
   e = cudaMemsetAsync(L.work_counter, 0, sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
   if (marks) cudaEventRecord(marks[0], st);
-  k_render_warp<CAPW><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
+  if (L.flags & kFlagBlueNoise)
+    k_render_warp<CAPW, true><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
+  else
+    k_render_warp<CAPW, false><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (marks) cudaEventRecord(marks[1], st);
@@ -1434,7 +1613,7 @@ cudaError_t launch_warp(const RenderLaunch& L, cudaStream_t st, const cudaEvent_
 }  // namespace
 
 bool render_uses_warp_kernel(const RenderLaunch& L) {
-  return L.traversal == AARBF_TRAVERSAL_AUTO && (L.flags & kFlagMajorantTracking) && !(L.flags & kFlagBlueNoise);
+  return L.traversal == AARBF_TRAVERSAL_AUTO && ((L.flags & kFlagMajorantTracking) || (L.flags & kFlagBlueNoise));
 }
 
 cudaError_t render_warp_stack_words(size_t* words) {

@@ -195,19 +195,44 @@ def test_render_flags(ctx, orc, aarbf_mod, flags_extra, kw):
     assert_radiance(ga, oa, "accum")
 
 
-@pytest.mark.parametrize("traversal", [0, 1])
-def test_render_marching_blue_noise(ctx, orc, aarbf_mod, traversal):
+@pytest.mark.parametrize("traversal,unit_scale", [(0, 0.1), (1, 0.1), (2, 0.1), (0, 0.004)])
+def test_render_marching_blue_noise(ctx, orc, aarbf_mod, traversal, unit_scale):
+    """stochastic marching: one warp per ray (0), point queries (1), one thread per ray (2); the
+    tiny unit makes rays run out of the 10000-step budget"""
     xyzw, _ = random_scene(10_000, 14)
     dom = orc.domain([xyzw])
     w, h = 40, 24
     rp, r = reference_params(aarbf_mod, dom, w, h, spp=2, traversal=traversal,
                              flags=aarbf_mod.FLAG_VISUALIZE_ATTRIBUTES | aarbf_mod.FLAG_BLUE_NOISE)
+    rp.unit = float(np.float32(r * unit_scale))
     scene, *_ = setup_both(ctx, orc, aarbf_mod, xyzw, None, 1, r)
     atlas = aarbf_mod.generate_noise_atlas()
     ctx.set_noise_atlas(atlas)
     ga, gi = gpu_render(ctx, rp, w, h)
     oa, oi = scene.render(orc.params_from(rp, noise=atlas), w, h)
     assert_radiance(gi, oi, "image")
+    assert (oi[..., :3] > 0).mean() > 0.01
+
+
+@pytest.mark.parametrize("traversal", [0, 2])
+def test_render_marching_native_dense(ctx, orc, aarbf_mod, traversal):
+    """native-mode marching (per-particle radii, linear density) through dense clusters: the warp
+    tracker's staging overflows and falls back to shorter chunks and direct steps"""
+    from aarbf import scenes
+    sc = scenes.config_clusters(60_000, clusters=8, seed=19)
+    cm, rm, dm = scenes.tf_linear_ramp()
+    dom = orc.domain([sc.xyzw])
+    w, h = 32, 24
+    rp = scenes.native_params(scenes.orbit_camera(), w, h, float(sc.radii.max()), 0.002, 400.0, dom, spp=2,
+                              marching=True, traversal=traversal)
+    scene, *_ = setup_both(ctx, orc, aarbf_mod, sc.xyzw, sc.radii, 4, rp.rbf_radius, tf32=(cm, rm, dm))
+    atlas = aarbf_mod.generate_noise_atlas()
+    ctx.set_noise_atlas(atlas)
+    ga, gi = gpu_render(ctx, rp, w, h)
+    oa, oi = scene.render(orc.params_from(rp, noise=atlas), w, h)
+    assert_radiance(gi, oi, "image")
+    assert_radiance(ga, oa, "accum")
+    assert (oi[..., :3] > 0).mean() > 0.01
 
 
 @pytest.mark.parametrize("traversal", [0, 1])
