@@ -75,6 +75,7 @@ def parse():
                     help="scenes of the batched-rendering measurement (0: skip)")
     ap.add_argument("--precision-particles", type=int, default=100_000_000,
                     help="particles of the fp32/FP16 storage comparison (0: skip)")
+    ap.add_argument("--series-frames", type=int, default=6, help="frames of the series-playback measurement (0: skip)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
@@ -557,6 +558,42 @@ def batched_timing(args, dev, stream):
             "speedup_vs_plain": (rays / t_graph) / (pr / t_plain)}
 
 
+def series_timing(args, sc, xyzw_pin, radii_pin, tf, dom, rmax, dev):
+    """Playback of a series of series_frames frames (the benchmark scene drifting by 0.001 per
+    frame along x) at 1 spp per frame: the reference's order (upload, build, render, one after
+    the other) against the overlapped pipeline of aarbf.streaming (upload and build of frame k+1
+    during the render of frame k). Device-event time over the whole series."""
+    import torch
+    from aarbf import streaming
+    W, H = args.width, args.height
+    frames = [(xyzw_pin, radii_pin)]
+    for k in range(1, args.series_frames):
+        x = sc.xyzw.copy()
+        x[:, 0] += np.float32(0.001 * k)
+        frames.append((torch.from_numpy(x).pin_memory(), radii_pin))
+    accum = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)
+    imgs = [torch.zeros((H, W, 4), dtype=torch.float32, device=dev) for _ in frames]
+
+    def params(k):
+        return params_for(args, dom, rmax, frame_id=k, spp=1)
+
+    out = {"frames": len(frames), "spp": 1}
+    sr = streaming.SeriesRenderer(dev.index or 0, dom, tf, rmax, ppl=args.ppl, alpha_floor=args.alpha_floor)
+    sr.render_series(frames[:2], params, W, H, accum, imgs[:2])  # warm-up (allocations)
+    for overlap in (False, True):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sr.render_series(frames, params, W, H, accum, imgs, overlap=overlap)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out["overlapped" if overlap else "sequential"] = {"ms_per_frame": dt / len(frames) * 1e3,
+                                                          "frames_s": len(frames) / dt}
+    sr.close()
+    out["speedup"] = out["overlapped"]["frames_s"] / out["sequential"]["frames_s"]
+    out["timing"] = "host wall clock around the whole series (uploads, builds and renders of every frame)"
+    return out
+
+
 def variant_timings(ctx, args, dom, rmax, accum, image, stream):
     """The other estimators of the benchmark configuration's frame, each timed with CUDA events
     on the launching stream after one warm-up launch (untimed by the headline figure):
@@ -739,6 +776,8 @@ def main():
                "steps": k_e2e, "ms_per_step": te / k_e2e * 1e3}
 
     variants = None if args.no_variants else variant_timings(ctx, args, dom, rmax, accum, image, stream)
+    series = (series_timing(args, sc, xyzw_pin, radii_pin, tf, dom, rmax, dev)
+              if args.series_frames > 1 and world == 1 else None)
     diff = differentiable_timing(args, dev, stream) if args.diff_views > 0 and world == 1 else None
     batched = batched_timing(args, dev, stream) if args.batch_scenes > 0 and world == 1 else None
     precision = precision_timing(args, dev, stream) if args.precision_particles > 0 and world == 1 else None
@@ -774,7 +813,7 @@ def main():
                          "accumulate_ms": accumulate_ms / max(timed_renders, 1), "kernel_counters": counts},
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": 2 * timed_renders,
             "build_ms": build_s * 1e3, "plain_estimator": plain, "variants": variants, "equal_rmse": rmse,
-            "differentiable": diff, "batched": batched, "precision": precision,
+            "differentiable": diff, "batched": batched, "precision": precision, "series": series,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
