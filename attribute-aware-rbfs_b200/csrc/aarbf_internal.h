@@ -98,7 +98,10 @@ cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt,
                              uint64_t n, int key_bits, uint32_t* hist, size_t hist_words,
                              cudaStream_t st, bool* result_in_alt);
 size_t radix_sort_hist_words(uint64_t n);
-cudaError_t launch_tie_check(const uint64_t* keys, uint64_t n, uint32_t* flag, cudaStream_t st);
+// orders every run of equal sorted keys of at most 64 entries by (x, y, z, w, input index) in
+// place on perm; *flag |= 1 if any run exists, |= 2 if a longer run needs the full chain
+cudaError_t launch_tie_runs(const uint64_t* keys, const float4* p, uint32_t* perm, uint64_t n, uint32_t* flag,
+                            cudaStream_t st);
 cudaError_t launch_orderable_component(const float4* p, const uint32_t* perm, uint64_t n, int comp,
                                        uint64_t* out, cudaStream_t st);
 cudaError_t launch_hilbert_keys_perm(const float4* p, const uint32_t* perm, uint64_t n, const float* dom,

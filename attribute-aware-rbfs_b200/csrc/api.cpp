@@ -549,13 +549,14 @@ aarbf_status aarbf_build(aarbf_ctx* ctx, float rbf_radius, uint32_t ppl, void* s
       keys = ctx->keys_alt.as<uint64_t>();
       perm = ctx->perm_alt.as<uint32_t>();
     }
-    // equal keys: redo as an LSD chain over (w, z, y, x) then the key, each pass stable
+    // equal keys: short runs are ordered in place; a run longer than the in-place limit redoes
+    // the sort as an LSD chain over (w, z, y, x) then the key, each pass stable
     CK(cudaMemsetAsync(ctx->flag.ptr, 0, 4, st), "flag");
-    CK(launch_tie_check(keys, n, ctx->flag.as<uint32_t>(), st), "tie check");
+    CK(launch_tie_runs(keys, in, perm, n, ctx->flag.as<uint32_t>(), st), "tie runs");
     uint32_t tie = 0;
     CK(cudaMemcpyAsync(&tie, ctx->flag.ptr, 4, cudaMemcpyDeviceToHost, st), "tie read");
     CK(cudaStreamSynchronize(st), "tie sync");
-    if (tie) {
+    if (tie & 2u) {
       uint64_t* k0 = ctx->keys.as<uint64_t>();
       uint64_t* k1 = ctx->keys_alt.as<uint64_t>();
       uint32_t* p0 = ctx->perm.as<uint32_t>();

@@ -78,8 +78,8 @@ extern "C" aarbf_status aarbf_hilbert_sort_noalloc(const float* xyzw, uint64_t n
   const float4* in = reinterpret_cast<const float4*>(xyzw);
   if (radix_sort_hist_words(n) > kHistWords) return AARBF_ERR_INVALID_ARGUMENT;
 
-  // same steps as aarbf_build: keys + identity, 48-bit radix sort, tie check, and on ties the
-  // stable LSD chain over (w, z, y, x) then the key
+  // same steps as aarbf_build: keys + identity, 48-bit radix sort, short runs of equal keys
+  // ordered in place, and for a longer run the stable LSD chain over (w, z, y, x) then the key
   bool alt = false;
   if (launch_hilbert_keys(in, n, dom, keys, perm, st) != cudaSuccess) return AARBF_ERR_CUDA;
   if (radix_sort_pairs(keys, perm, keys_alt, perm_alt, n, 48, hist, kHistWords, st, &alt) != cudaSuccess)
@@ -90,11 +90,11 @@ extern "C" aarbf_status aarbf_hilbert_sort_noalloc(const float* xyzw, uint64_t n
       return AARBF_ERR_CUDA;
   }
   uint32_t tie = 0;
-  if (cudaMemsetAsync(flag, 0, 4, st) != cudaSuccess || launch_tie_check(keys, n, flag, st) != cudaSuccess ||
+  if (cudaMemsetAsync(flag, 0, 4, st) != cudaSuccess || launch_tie_runs(keys, in, perm, n, flag, st) != cudaSuccess ||
       cudaMemcpyAsync(&tie, flag, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return AARBF_ERR_CUDA;
-  if (!tie) return AARBF_OK;
+  if (!(tie & 2u)) return AARBF_OK;
   uint64_t *k0 = keys, *k1 = keys_alt;
   uint32_t *p0 = perm, *p1 = perm_alt;
   if (launch_hilbert_keys(in, n, dom, k0, p0, st) != cudaSuccess) return AARBF_ERR_CUDA;

@@ -1,7 +1,8 @@
 // preprocess.cu -- device side of the reference's host preprocessing (hostCode.cpp:183-250):
 // space-time domain reduction, 16-bit quantisation + 3-D Hilbert keys, a stable LSD radix
-// sort (hand written: per-tile histogram, exclusive scan, stable warp-multisplit scatter),
-// the lexicographic tie-break pass and the gather that normalises attributes.
+// sort (hand written: per-tile histogram, exclusive scan, stable warp-multisplit scatter through
+// shared memory), the in-place ordering of equal-key runs (the lexicographic LSD chain for long
+// runs) and the gather that normalises attributes.
 #include <cfloat>
 
 #include "aarbf_internal.h"
@@ -99,10 +100,53 @@ __global__ void k_orderable(const float4* __restrict__ p, const uint32_t* __rest
   out[i] = orderable(f);
 }
 
-__global__ void k_tie_check(const uint64_t* __restrict__ keys, uint64_t n, uint32_t* flag) {
-  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+// (x, y, z, w, input index) of particle a before that of particle b, each coordinate compared as
+// floats compare (orderable() maps +0 and -0 together)
+__device__ __forceinline__ bool tie_less(float4 a, uint32_t ia, float4 b, uint32_t ib) {
+  uint32_t ua = orderable(a.x), ub = orderable(b.x);
+  if (ua != ub) return ua < ub;
+  ua = orderable(a.y), ub = orderable(b.y);
+  if (ua != ub) return ua < ub;
+  ua = orderable(a.z), ub = orderable(b.z);
+  if (ua != ub) return ua < ub;
+  ua = orderable(a.w), ub = orderable(b.w);
+  if (ua != ub) return ua < ub;
+  return ia < ib;
+}
+
+// Runs of equal keys after the stable key sort from the identity hold their particles in input
+// order. The reference sorts (key, float4) pairs (hostCode.cpp:212-222), so equal keys are
+// ordered by x, then y, z, w; equal particles keep input order here. The thread at the start of
+// each run sorts a run of at most kMaxTieRun entries in place (insertion sort on perm); a longer
+// run sets bit 1 of *flag and is left to the full LSD chain over (w, z, y, x, key). Bit 0 is set
+// when any run exists.
+constexpr int kMaxTieRun = 64;
+
+__global__ void k_tie_runs(const uint64_t* __restrict__ keys, const float4* __restrict__ p,
+                           uint32_t* __restrict__ perm, uint64_t n, uint32_t* flag) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i + 1 >= n) return;
-  if (keys[i] == keys[i + 1]) atomicOr(flag, 1u);
+  const uint64_t k = keys[i];
+  if (keys[i + 1] != k || (i > 0 && keys[i - 1] == k)) return;
+  uint64_t e = i + 2;
+  while (e < n && e - i <= (uint64_t)kMaxTieRun && keys[e] == k) ++e;
+  if (e - i > (uint64_t)kMaxTieRun) {
+    atomicOr(flag, 3u);
+    return;
+  }
+  atomicOr(flag, 1u);
+  for (uint64_t a = i + 1; a < e; ++a) {
+    const uint32_t v = perm[a];
+    const float4 q = __ldg(p + v);
+    uint64_t b = a;
+    while (b > i) {
+      const uint32_t u = perm[b - 1];
+      if (!tie_less(q, v, __ldg(p + u), u)) break;
+      perm[b] = u;
+      --b;
+    }
+    perm[b] = v;
+  }
 }
 
 __global__ void k_gather_normalize(const float4* __restrict__ in, const float* __restrict__ rin,
@@ -126,10 +170,14 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_hist(const uint64_t* __r
   h[threadIdx.x] = 0;
   __syncthreads();
   uint64_t base = (uint64_t)blockIdx.x * kSortTile;
+  const uint32_t lt = lanemask_lt();
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
     uint64_t idx = base + (uint64_t)k * kSortThreads + threadIdx.x;
-    if (idx < n) atomicAdd(&h[(uint32_t)(keys[idx] >> shift) & 255u], 1u);
+    // equal digits of a warp add once (clustered keys share their upper digits)
+    uint32_t d = idx < n ? ((uint32_t)(keys[idx] >> shift) & 255u) : 256u;
+    uint32_t peers = __match_any_sync(0xffffffffu, d);
+    if (d < 256u && (peers & lt) == 0) atomicAdd(&h[d], (uint32_t)__popc(peers));
   }
   __syncthreads();
   hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
@@ -210,19 +258,27 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(uint32_t* __restric
 }
 
 // stable scatter: warp w of a tile owns keys [w*256, (w+1)*256) of the tile and walks them in
-// 8 batches of 32 in input order; ranks inside a batch come from __match_any_sync.
+// 8 batches of 32 in input order; ranks inside a batch come from __match_any_sync. The tile is
+// first reordered by digit in shared memory, then written out by consecutive threads, so that a
+// warp's stores fall into few runs of consecutive addresses (one per digit it covers).
 __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(
     const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint64_t* __restrict__ kout,
     uint32_t* __restrict__ vout, uint64_t n, int shift, const uint32_t* __restrict__ offs, uint32_t ntiles) {
   constexpr int kWarps = kSortThreads / 32;
+  static_assert(kSortThreads == 256, "one thread per digit");
   __shared__ uint32_t cnt[kWarps][256];
   __shared__ uint32_t gofs[256];
+  __shared__ uint32_t lstart[256];
+  __shared__ uint32_t ws[32];
+  __shared__ uint64_t sk[kSortTile];
+  __shared__ uint32_t sv[kSortTile];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int w = 0; w < kWarps; ++w) cnt[w][threadIdx.x] = 0;
   gofs[threadIdx.x] = offs[(uint64_t)threadIdx.x * ntiles + blockIdx.x];
   __syncthreads();
-  const uint64_t base = (uint64_t)blockIdx.x * kSortTile + (uint64_t)warp * (32 * kSortItems);
+  const uint64_t tile0 = (uint64_t)blockIdx.x * kSortTile;
+  const uint64_t base = tile0 + (uint64_t)warp * (32 * kSortItems);
   uint64_t k[kSortItems];
   uint32_t v[kSortItems], pos[kSortItems], dig[kSortItems];
   const uint32_t lt = lanemask_lt();
@@ -243,22 +299,35 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(
     pos[b] = before + rank;
   }
   __syncthreads();
-  {
-    uint32_t run = 0;
+  // per digit (thread = digit): exclusive prefix over the warps, then over the digits
+  uint32_t run = 0;
 #pragma unroll
-    for (int w = 0; w < kWarps; ++w) {
-      uint32_t c = cnt[w][threadIdx.x];
-      cnt[w][threadIdx.x] = run;
-      run += c;
-    }
+  for (int w = 0; w < kWarps; ++w) {
+    uint32_t c = cnt[w][threadIdx.x];
+    cnt[w][threadIdx.x] = run;
+    run += c;
   }
+  uint32_t tile_total;
+  lstart[threadIdx.x] = block_exclusive_scan(run, ws, &tile_total);
   __syncthreads();
 #pragma unroll
   for (int b = 0; b < kSortItems; ++b) {
     if (dig[b] < 256u) {
-      uint32_t dst = gofs[dig[b]] + cnt[warp][dig[b]] + pos[b];
-      kout[dst] = k[b];
-      vout[dst] = v[b];
+      uint32_t lp = lstart[dig[b]] + cnt[warp][dig[b]] + pos[b];
+      sk[lp] = k[b];
+      sv[lp] = v[b];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    uint32_t j = (uint32_t)r * kSortThreads + threadIdx.x;
+    if (j < tile_total) {
+      uint64_t key = sk[j];
+      uint32_t d = (uint32_t)(key >> shift) & 255u;
+      uint32_t dst = gofs[d] + (j - lstart[d]);
+      kout[dst] = key;
+      vout[dst] = sv[j];
     }
   }
 }
@@ -327,9 +396,10 @@ cudaError_t launch_hilbert_keys_perm(const float4* p, const uint32_t* perm, uint
   return cudaGetLastError();
 }
 
-cudaError_t launch_tie_check(const uint64_t* keys, uint64_t n, uint32_t* flag, cudaStream_t st) {
+cudaError_t launch_tie_runs(const uint64_t* keys, const float4* p, uint32_t* perm, uint64_t n, uint32_t* flag,
+                            cudaStream_t st) {
   if (n < 2) return cudaSuccess;
-  k_tie_check<<<blocks_for(n, 256), 256, 0, st>>>(keys, n, flag);
+  k_tie_runs<<<blocks_for(n, 256), 256, 0, st>>>(keys, p, perm, n, flag);
   return cudaGetLastError();
 }
 

@@ -558,6 +558,32 @@ def batched_timing(args, dev, stream):
             "speedup_vs_plain": (rays / t_graph) / (pr / t_plain)}
 
 
+def build_timing(ctx, args, rmax, n, stream, reps=3):
+    """Steady-state rebuild of the benchmark scene (particles already on the device, buffers
+    reserved): Hilbert keys, 48-bit radix sort, ordering of equal-key runs, gather + attribute
+    normalisation, Karras LBVH, refit, wide-node collapse and the largest-radius reduction.
+    Device time between CUDA events on the build's stream (the build's one host read-back of the
+    tie flag sits inside it). Algorithmic bytes: n * (20 B record + 8 B key) + 6 radix passes *
+    2 * (8 B key + 4 B index) * n + 2 * ceil(n / ppl) nodes * 32 B."""
+    import torch
+    peak, kind = measured_peak()
+    ms = []
+    for _ in range(reps + 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.build(rmax, args.ppl, stream=stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    ms = ms[1:]
+    nl = -(-n // args.ppl)
+    b_alg = n * (20 + 8) + 6 * 2 * 12 * n + 2 * nl * 32
+    t = sum(ms) / len(ms)
+    ach = b_alg / (t * 1e-3) / 1e9
+    return {"ms": t, "ms_runs": ms, "particles": n, "algorithmic_bytes": b_alg, "achieved_gbs": ach,
+            "frac": ach / peak, "peak": peak, "peak_kind": kind}
+
+
 def series_timing(args, sc, xyzw_pin, radii_pin, tf, dom, rmax, dev):
     """Playback of a series of series_frames frames (the benchmark scene drifting by 0.001 per
     frame along x) at 1 spp per frame: the reference's order (upload, build, render, one after
@@ -776,6 +802,7 @@ def main():
                "steps": k_e2e, "ms_per_step": te / k_e2e * 1e3}
 
     variants = None if args.no_variants else variant_timings(ctx, args, dom, rmax, accum, image, stream)
+    build = build_timing(ctx, args, rmax, int(sc.xyzw.shape[0]), stream) if world == 1 else None
     series = (series_timing(args, sc, xyzw_pin, radii_pin, tf, dom, rmax, dev)
               if args.series_frames > 1 and world == 1 else None)
     diff = differentiable_timing(args, dev, stream) if args.diff_views > 0 and world == 1 else None
@@ -812,7 +839,7 @@ def main():
                          else "k_render", "kernel_ms": launch_s * 1e3,
                          "accumulate_ms": accumulate_ms / max(timed_renders, 1), "kernel_counters": counts},
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": 2 * timed_renders,
-            "build_ms": build_s * 1e3, "plain_estimator": plain, "variants": variants, "equal_rmse": rmse,
+            "build_ms": build_s * 1e3, "build": build, "plain_estimator": plain, "variants": variants, "equal_rmse": rmse,
             "differentiable": diff, "batched": batched, "precision": precision, "series": series,
         }
         print(json.dumps(line), flush=True)

@@ -101,7 +101,8 @@ def setup_both(ctx, orc, aarbf_mod, xyzw, radii, ppl, rbf, tf8=None, tf32=None, 
 
 
 @pytest.mark.parametrize("n,ppl,dup", [(1, 1, 0), (2, 1, 0), (7, 4, 0), (1000, 1, 0), (1000, 16, 40),
-                                       (50_000, 1, 0), (50_000, 8, 500), (3, 8, 0)])
+                                       (50_000, 1, 0), (50_000, 8, 500), (3, 8, 0),
+                                       (200_000, 1, 60)])
 def test_build_bitexact(ctx, orc, aarbf_mod, n, ppl, dup):
     xyzw, radii = random_scene(n, seed=n + ppl, dup=dup, radii=(ppl == 8))
     scene, keys, perm, dom = setup_both(ctx, orc, aarbf_mod, xyzw, radii, ppl, 0.02)
