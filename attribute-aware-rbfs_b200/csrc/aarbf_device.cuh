@@ -217,12 +217,16 @@ __device__ __forceinline__ uint64_t hilbert3x16(uint64_t c0, uint64_t c1, uint64
   // OR-packing lets a coordinate equal to 65536 spill into the next axis field, as in the
   // reference; bits above 48 are dropped by the transpose
   uint64_t packed = (((c2 << 16) | c1) << 16) | c0;
+  // bit b of field d goes to bit 3b + d (the reference's bitTranspose), spread by masks
   uint64_t inter = 0;
 #pragma unroll
   for (unsigned d = 0; d < 3; ++d) {
-    uint64_t field = (packed >> (d * 16)) & 0xffffull;
-#pragma unroll
-    for (unsigned b = 0; b < 16; ++b) inter |= ((field >> b) & 1ull) << (b * 3 + d);
+    uint64_t x = (packed >> (d * 16)) & 0xffffull;
+    x = (x | (x << 16)) & 0x0000ff0000ffull;
+    x = (x | (x << 8)) & 0x00f00f00f00full;
+    x = (x | (x << 4)) & 0x0c30c30c30c3ull;
+    x = (x | (x << 2)) & 0x249249249249ull;
+    inter |= x << d;
   }
   inter ^= inter >> 3;
   uint64_t index = 0;

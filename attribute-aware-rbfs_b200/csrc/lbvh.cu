@@ -164,9 +164,11 @@ __global__ void k_refit(const float4* __restrict__ rec0, const float* __restrict
     int slot = (pn->d.x == child) ? 0 : 1;
     write_slot(pn, slot, elo, ehi);
     write_slot(pr, slot, lo, hi);
-    __threadfence();
+    // release the slot before the arrival count, acquire the sibling's slot after it
+    // (acquire-release fences: the message-passing pattern needs no sequentially consistent fence)
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
     if (atomicAdd(counters + parent, 1u) == 0u) return;
-    __threadfence();
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
     read_union(pn, elo, ehi);
     read_union(pr, lo, hi);
     uint32_t up = pn->d.z;

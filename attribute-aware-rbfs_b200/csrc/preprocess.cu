@@ -170,14 +170,10 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_hist(const uint64_t* __r
   h[threadIdx.x] = 0;
   __syncthreads();
   uint64_t base = (uint64_t)blockIdx.x * kSortTile;
-  const uint32_t lt = lanemask_lt();
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
     uint64_t idx = base + (uint64_t)k * kSortThreads + threadIdx.x;
-    // equal digits of a warp add once (clustered keys share their upper digits)
-    uint32_t d = idx < n ? ((uint32_t)(keys[idx] >> shift) & 255u) : 256u;
-    uint32_t peers = __match_any_sync(0xffffffffu, d);
-    if (d < 256u && (peers & lt) == 0) atomicAdd(&h[d], (uint32_t)__popc(peers));
+    if (idx < n) atomicAdd(&h[(uint32_t)(keys[idx] >> shift) & 255u], 1u);
   }
   __syncthreads();
   hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
