@@ -317,7 +317,8 @@ struct Stager {
 
 // Count mode (roofline accounting, not timed): the particles whose sphere meets the traversed
 // segment [t0, t1] of a ray (exact test, no slack) and the BVH nodes a segment query visits.
-__device__ void count_segment(const RenderLaunch& L, const Ray& ray, float t0, float t1) {
+// out of line: count mode only, kept out of the tracking kernels' instruction stream and frame
+__device__ __noinline__ void count_segment(const RenderLaunch& L, const Ray& ray, float t0, float t1) {
   const SceneView& s = L.s;
   if (s.nleaves == 0 || !(t1 >= t0)) return;
   const float3 inv = make_float3(1.0f / ray.d.x, 1.0f / ray.d.y, 1.0f / ray.d.z);
@@ -696,8 +697,9 @@ __device__ __forceinline__ void track(const RenderLaunch& L, Tracker& tr, const 
 }
 
 // ParticleRBFRayGen body for one sample (deviceCodeRBF.hlsl:206-324); track_fn runs the tracker
-// (per thread or per warp), count_lane selects the lane that does count-mode accounting
-template <class TrackFn>
+// (per thread or per warp), count_lane selects the lane that does count-mode accounting. BLUE:
+// the blue-noise flag when the caller knows it at compile time (0 or 1), else -1 (read from L)
+template <int BLUE = -1, class TrackFn>
 __device__ float4 raygen_generic(const RenderLaunch& L, uint32_t frame, int px, int py, float& noise,
                                  bool count_lane, TrackFn&& track_fn) {
   uint32_t rng = pixel_seed(frame, (uint32_t)px, (uint32_t)py, (uint32_t)L.width);
@@ -719,7 +721,7 @@ __device__ float4 raygen_generic(const RenderLaunch& L, uint32_t frame, int px, 
   aabb_clip(ray.o, ray.d, lb, rt, ray.tmin, ray.tmax, tenter, texit);
 
   Tracker tr;
-  const bool blue = (L.flags & kFlagBlueNoise) != 0;
+  const bool blue = BLUE >= 0 ? BLUE != 0 : (L.flags & kFlagBlueNoise) != 0;
   float r0;
   if (blue) {
     uint32_t gx = frame % 8u, gy = (frame / 8u) % 16u;
@@ -818,6 +820,13 @@ struct WarpBuf {
   uint32_t leaves[64];
 };
 
+// this warp's buffer, addressed in the shared window (out-of-line functions receiving the buffer
+// as a generic pointer would reach it with generic loads and stores)
+template <int CAPW>
+__device__ __forceinline__ WarpBuf<CAPW>* warp_buf() {
+  extern __shared__ __align__(16) char smem[];
+  return reinterpret_cast<WarpBuf<CAPW>*>(smem) + (threadIdx.x >> 5);
+}
 
 __device__ __forceinline__ void warp_sum_sample(Sample& s) {
   s.count = warp_sum(s.count);
@@ -1025,10 +1034,11 @@ template <int CAPW>
 __device__ __noinline__ long long warp_bin_sum_direct(const SceneView& s, const Ray ray, const float3 inv, float lo,
                                                       float hi, WarpBuf<CAPW>* buf, uint32_t* stk, uint32_t* status,
                                                       unsigned long long* ctr) {
+  (void)buf;
   long long acc = 0;
   const float eps = s.eps;
   warp_traverse(
-      s, stk, buf->leaves, status,
+      s, stk, warp_buf<CAPW>()->leaves, status,
       [&](float lx, float ly, float lz, float hx, float hy, float hz) {
         return seg_box(lx, ly, lz, hx, hy, hz, ray.o, inv, lo, hi, eps);
       },
@@ -1045,10 +1055,11 @@ __device__ __noinline__ long long warp_bin_sum_direct(const SceneView& s, const 
 template <int CAPW>
 __device__ __noinline__ Sample warp_point(const SceneView& s, const float3 x, WarpBuf<CAPW>* buf, uint32_t* stk,
                                           uint32_t* status, unsigned long long* ctr) {
+  (void)buf;
   Sample acc;
   sample_clear(acc);
   warp_traverse(
-      s, stk, buf->leaves, status,
+      s, stk, warp_buf<CAPW>()->leaves, status,
       [&](float lx, float ly, float lz, float hx, float hy, float hz) { return inside(lx, ly, lz, hx, hy, hz, x); },
       [&](bool v, uint32_t i) -> bool {
         if (v) eval_particle(s, i, x, acc);
@@ -1192,9 +1203,10 @@ __device__ __noinline__
 #endif
 void track_majorant_warp(const RenderLaunch& L, Tracker& tr_io, const Ray& ray_io,
                                                  WarpBuf<CAPW>* buf, uint32_t* stk) {
+  (void)buf;  // the same buffer, addressed as shared memory
   Tracker tr = tr_io;
   const Ray ray = ray_io;
-  track_majorant_warp_body<CAPW>(L, tr, ray, buf, stk);
+  track_majorant_warp_body<CAPW>(L, tr, ray, warp_buf<CAPW>(), stk);
   tr_io = tr;
 }
 
@@ -1358,9 +1370,10 @@ __device__ __forceinline__ void track_march_warp_body(const RenderLaunch& L, Tra
 template <int CAPW>
 __device__ __noinline__ void track_march_warp(const RenderLaunch& L, Tracker& tr_io, const Ray& ray_io,
                                               WarpBuf<CAPW>* buf, uint32_t* stk) {
+  (void)buf;  // the same buffer, addressed as shared memory
   Tracker tr = tr_io;
   const Ray ray = ray_io;
-  track_march_warp_body<CAPW>(L, tr, ray, buf, stk);
+  track_march_warp_body<CAPW>(L, tr, ray, warp_buf<CAPW>(), stk);
   tr_io = tr;
 }
 
@@ -1391,7 +1404,7 @@ __device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t
   const size_t ofs = (size_t)px + (size_t)L.width * (size_t)py;
   const long long c0 = cost ? clock64() : 0;
   float noise = 0.0f;
-  float4 c = raygen_generic(L, (L.frame_id + k) & 0xffffu, px, py, noise, lane == 0,
+  float4 c = raygen_generic<MARCH ? 1 : 0>(L, (L.frame_id + k) & 0xffffu, px, py, noise, lane == 0,
                             [&](Tracker& tr, const Ray& r, bool) {
                               if (MARCH) track_march_warp<CAPW>(L, tr, r, buf, stk);
                               else track_majorant_warp<CAPW>(L, tr, r, buf, stk);
