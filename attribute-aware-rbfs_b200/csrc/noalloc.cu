@@ -1,8 +1,8 @@
 // noalloc.cu -- an allocation-free variant of the Hilbert-key sort that aarbf_build runs.
 //
-// Some callers cannot call cudaMalloc: code that runs while a CUDA graph is being captured
-// around it, callers whose memory is managed by a pool or arena that forbids side allocations,
-// and real-time render loops that must not hit the allocator (or its implicit synchronisation)
+// Some callers cannot call cudaMalloc: applications whose device memory is handed out by their
+// own pool or arena, which forbids allocations made behind its back, and real-time render loops
+// that must not reach the allocator (cudaMalloc and cudaFree can synchronise the whole device)
 // once they are running. aarbf_hilbert_sort_noalloc serves them: the caller passes the particles
 // and the two outputs; the sort's working space (the radix sort's second key/index buffers, its
 // histograms and a flag) is one file-scope __device__ array of a fixed size, so nothing is

@@ -281,11 +281,11 @@ aarbf_status aarbf_series_save(const char *path, const float *const *frames, con
 
 /* ---- allocation-free Hilbert sort ---------------------------------------------------------- */
 
-/* No counterpart in the reference. For callers that cannot allocate device memory -- code run
- * while a CUDA graph is being captured, memory managed by a pool or arena that forbids other
- * allocations, real-time loops that must not touch the allocator: the Hilbert keys and sort
- * permutation that aarbf_build computes, without calling cudaMalloc or cudaFree. xyzw: device
- * pointer to n float4 particles; dom: HOST pointer to the 8-float domain of aarbf_set_domain;
+/* No counterpart in the reference. For callers that cannot allocate device memory -- device
+ * memory handed out by the application's own pool or arena, which forbids other allocations,
+ * real-time loops that must not reach the allocator (it can synchronise the device): the
+ * Hilbert keys and sort permutation that aarbf_build computes, without calling cudaMalloc or
+ * cudaFree. xyzw: device pointer to n float4 particles; dom: HOST pointer to the 8-float domain of aarbf_set_domain;
  * keys (n x u64) and perm (n x u32): device outputs, equal to aarbf_get_hilbert_keys' results.
  * Working space is a fixed array in device memory that every GPU loading the library holds
  * until the process exits (about 12.5 MiB), so n is limited to AARBF_NOALLOC_MAX_PARTICLES;

@@ -1,8 +1,8 @@
 """The allocation-free Hilbert sort (aarbf_hilbert_sort_noalloc) against the sort aarbf_build runs.
 
-This entry point exists for callers that cannot allocate device memory while they run -- work
-recorded into a CUDA graph, memory owned by a pool or arena, real-time loops that must not call
-the allocator. It keeps its working space in one fixed device array shared by every call. The test
+This entry point exists for callers that cannot allocate device memory while they run -- device
+memory owned by the application's pool or arena, real-time loops that must not call the
+allocator (it can synchronise the device). It keeps its working space in one fixed device array shared by every call. The test
 calls it through the C ABI twice in a row on different inputs (so leftovers of the first call in
 the shared array would show up in the second) and compares keys and permutation with
 aarbf_build's, which must match exactly (integer outputs). It also checks that sizes beyond the
