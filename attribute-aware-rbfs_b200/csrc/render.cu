@@ -1072,9 +1072,9 @@ __device__ __noinline__ Sample warp_point(const SceneView& s, const float3 x, Wa
 }
 
 // track_majorant with the warp-cooperative stager; same decisions, same random-number stream
-// out of line: one copy serves the primary and the shadow ray (instruction-cache footprint)
-// (the tracker state and the ray are copied into registers for the body: the caller's copies
-// live in local memory because their addresses cross the call)
+// out of line: one copy serves the primary and the shadow ray (instruction-cache footprint);
+// the tracker state and the ray cross the call by value (references would pin the caller's
+// copies in local memory)
 template <int CAPW>
 __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, Tracker& tr, const Ray& ray,
                                                          WarpBuf<CAPW>* buf, uint32_t* stk) {
@@ -1201,13 +1201,9 @@ __device__ __forceinline__
 #else
 __device__ __noinline__
 #endif
-void track_majorant_warp(const RenderLaunch& L, Tracker& tr_io, const Ray& ray_io,
-                                                 WarpBuf<CAPW>* buf, uint32_t* stk) {
-  (void)buf;  // the same buffer, addressed as shared memory
-  Tracker tr = tr_io;
-  const Ray ray = ray_io;
+Tracker track_majorant_warp(const RenderLaunch& L, Tracker tr, const Ray ray, uint32_t* stk) {
   track_majorant_warp_body<CAPW>(L, tr, ray, warp_buf<CAPW>(), stk);
-  tr_io = tr;
+  return tr;
 }
 
 // stochasticMarching (deviceCodeRBF.hlsl:67-139) with the warp: the steps of a chunk (up to 32)
@@ -1368,13 +1364,9 @@ __device__ __forceinline__ void track_march_warp_body(const RenderLaunch& L, Tra
 }
 
 template <int CAPW>
-__device__ __noinline__ void track_march_warp(const RenderLaunch& L, Tracker& tr_io, const Ray& ray_io,
-                                              WarpBuf<CAPW>* buf, uint32_t* stk) {
-  (void)buf;  // the same buffer, addressed as shared memory
-  Tracker tr = tr_io;
-  const Ray ray = ray_io;
+__device__ __noinline__ Tracker track_march_warp(const RenderLaunch& L, Tracker tr, const Ray ray, uint32_t* stk) {
   track_march_warp_body<CAPW>(L, tr, ray, warp_buf<CAPW>(), stk);
-  tr_io = tr;
+  return tr;
 }
 
 // persistent warps; an item is one sample of one pixel, ordered as in k_render
@@ -1406,8 +1398,8 @@ __device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t
   float noise = 0.0f;
   float4 c = raygen_generic<MARCH ? 1 : 0>(L, (L.frame_id + k) & 0xffffu, px, py, noise, lane == 0,
                             [&](Tracker& tr, const Ray& r, bool) {
-                              if (MARCH) track_march_warp<CAPW>(L, tr, r, buf, stk);
-                              else track_majorant_warp<CAPW>(L, tr, r, buf, stk);
+                              if (MARCH) tr = track_march_warp<CAPW>(L, tr, r, stk);
+                              else tr = track_majorant_warp<CAPW>(L, tr, r, stk);
                             });
   if (cost) c.w = (float)(clock64() - c0);
   if (lane == 0) {
