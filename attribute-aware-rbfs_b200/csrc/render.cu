@@ -318,7 +318,7 @@ struct Stager {
 // Count mode (roofline accounting, not timed): the particles whose sphere meets the traversed
 // segment [t0, t1] of a ray (exact test, no slack) and the BVH nodes a segment query visits.
 // out of line: count mode only, kept out of the tracking kernels' instruction stream and frame
-__device__ __noinline__ void count_segment(const RenderLaunch& L, const Ray& ray, float t0, float t1) {
+__device__ __noinline__ void count_segment(const RenderLaunch& L, const Ray ray, float t0, float t1) {
   const SceneView& s = L.s;
   if (s.nleaves == 0 || !(t1 >= t0)) return;
   const float3 inv = make_float3(1.0f / ray.d.x, 1.0f / ray.d.y, 1.0f / ray.d.z);
@@ -399,7 +399,7 @@ __device__ __forceinline__ float sample_density(const RenderLaunch& L, float D) 
 }
 
 // out of line: runs once per collision, and keeps three pow expansions out of the hot loops
-__device__ __noinline__ float3 sample_color(const RenderLaunch& L, const Sample& acc, float D) {
+__device__ __noinline__ float3 sample_color(const RenderLaunch& L, const Sample acc, float D) {
   if (L.flags & kFlagVisualizeAttributes) {
     const float g = 1.0f / 2.2f;
     float c0 = (float)acc.a1 * kFixInv, c1 = (float)acc.a2 * kFixInv, c2 = (float)acc.a3 * kFixInv;
