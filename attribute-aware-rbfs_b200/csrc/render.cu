@@ -1075,13 +1075,14 @@ __device__ __noinline__ Sample warp_point(const SceneView& s, const float3 x, Wa
 // out of line: one copy serves the primary and the shadow ray (instruction-cache footprint);
 // the tracker state and the ray cross the call by value (references would pin the caller's
 // copies in local memory)
-template <int CAPW>
+template <int CAPW, bool COUNT>
 __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, Tracker& tr, const Ray& ray,
                                                          WarpBuf<CAPW>* buf, uint32_t* stk) {
   WarpStager<CAPW> st;
   st.buf = buf;
   st.stk = stk;
-  st.ctr = L.counters;
+  unsigned long long* const ctr = COUNT ? L.counters : nullptr;  // count mode has its own instance
+  st.ctr = ctr;
   st.init(L.s, ray);
   const float Lb = L.bin_length;
   const float scale = L.density_scale;
@@ -1143,8 +1144,8 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
     float pend_hi[kSplitDepth];
     int pend_depth[kSplitDepth];
     for (;;) {
-      wctr(L.counters, kWcBins, 1);
-      long long acc = direct ? warp_bin_sum_direct<CAPW>(L.s, ray, st.inv, lo, hi, buf, stk, L.status, L.counters)
+      wctr(ctr, kWcBins, 1);
+      long long acc = direct ? warp_bin_sum_direct<CAPW>(L.s, ray, st.inv, lo, hi, buf, stk, L.status, ctr)
                              : st.bin_sum(L.s, ray, k, lo, hi);
       float M = ((float)acc * kFixInv) * minf;
       if (M > 0.0f) {
@@ -1164,14 +1165,14 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
             return;
           }
           tr.i += 1;
-          wctr(L.counters, kWcSteps, 1);
+          wctr(ctr, kWcSteps, 1);
           float u = lcg_f(tr.rng);
           float step = -dlog(1.0f - u) / M;
           t = t + step;
           if (t >= hi || t >= ray.tmax) break;
           float3 x = make_float3(ray.o.x + t * ray.d.x, ray.o.y + t * ray.d.y, ray.o.z + t * ray.d.z);
           Sample smp;
-          if (direct) smp = warp_point<CAPW>(L.s, x, buf, stk, L.status, L.counters);
+          if (direct) smp = warp_point<CAPW>(L.s, x, buf, stk, L.status, ctr);
           else st.sample(L.s, k, t, x, smp);
           float D = (float)smp.a0 * kFixInv;
           float sigma = D * scale;
@@ -1195,14 +1196,14 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
   tr.t = t;
 }
 
-template <int CAPW>
+template <int CAPW, bool COUNT>
 #if AARBF_TRACK_INLINE
 __device__ __forceinline__
 #else
 __device__ __noinline__
 #endif
 Tracker track_majorant_warp(const RenderLaunch& L, Tracker tr, const Ray ray, uint32_t* stk) {
-  track_majorant_warp_body<CAPW>(L, tr, ray, warp_buf<CAPW>(), stk);
+  track_majorant_warp_body<CAPW, COUNT>(L, tr, ray, warp_buf<CAPW>(), stk);
   return tr;
 }
 
@@ -1379,8 +1380,9 @@ __device__ __forceinline__ uint32_t warp_items(const RenderLaunch& L) {
 
 // one work item of the ray-per-warp kernel (all lanes of the warp); MARCH: stochastic marching
 // (blue-noise mode), else delta tracking with per-bin majorants, each in its own kernel so neither
-// carries the other's code
-template <int CAPW, bool MARCH>
+// carries the other's code; COUNT: the count-mode instance (render_count), so the timed instance
+// carries no accounting code
+template <int CAPW, bool MARCH, bool COUNT>
 __device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t item, WarpBuf<CAPW>* buf,
                                                  uint32_t* stk) {
   const uint32_t lane = threadIdx.x & 31u;
@@ -1396,10 +1398,10 @@ __device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t
   const size_t ofs = (size_t)px + (size_t)L.width * (size_t)py;
   const long long c0 = cost ? clock64() : 0;
   float noise = 0.0f;
-  float4 c = raygen_generic<MARCH ? 1 : 0>(L, (L.frame_id + k) & 0xffffu, px, py, noise, lane == 0,
+  float4 c = raygen_generic<MARCH ? 1 : 0>(L, (L.frame_id + k) & 0xffffu, px, py, noise, COUNT && lane == 0,
                             [&](Tracker& tr, const Ray& r, bool) {
                               if (MARCH) tr = track_march_warp<CAPW>(L, tr, r, stk);
-                              else tr = track_majorant_warp<CAPW>(L, tr, r, stk);
+                              else tr = track_majorant_warp<CAPW, COUNT>(L, tr, r, stk);
                             });
   if (cost) c.w = (float)(clock64() - c0);
   if (lane == 0) {
@@ -1408,7 +1410,7 @@ __device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t
   }
 }
 
-template <int CAPW, bool MARCH>
+template <int CAPW, bool MARCH, bool COUNT>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks) k_render_warp(const __grid_constant__ RenderLaunch L) {
   extern __shared__ __align__(16) char smem[];
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
@@ -1420,7 +1422,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks) k_render_
     if (lane == 0) item = atomicAdd(L.work_counter, 1u);
     item = __shfl_sync(kFull, item, 0);
     if (item >= total) break;
-    render_warp_item<CAPW, MARCH>(L, item, buf, stk);
+    render_warp_item<CAPW, MARCH, COUNT>(L, item, buf, stk);
   }
 }
 
@@ -1446,7 +1448,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks)
       if (item_ofs[mid] <= item) lo = mid;
       else hi = mid;
     }
-    render_warp_item<CAPW, false>(Ls[lo], (uint32_t)(item - item_ofs[lo]), buf, stk);
+    render_warp_item<CAPW, false, false>(Ls[lo], (uint32_t)(item - item_ofs[lo]), buf, stk);
   }
 }
 
@@ -1576,16 +1578,21 @@ cudaError_t warp_grid(int* blocks) {
   if (!cached) {
     const size_t smem = sizeof(WarpBuf<CAPW>) * kWarpsPerBlock;
     cudaError_t e =
-        cudaFuncSetAttribute(k_render_warp<CAPW, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_render_warp<CAPW, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_render_warp<CAPW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      e = cudaFuncSetAttribute(k_render_warp<CAPW, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_render_warp<CAPW, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0, per_sm = 0, per_m = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_warp<CAPW, false>, kWarpsPerBlock * 32, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_warp<CAPW, false, false>, kWarpsPerBlock * 32,
+                                                      smem);
     if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_m, k_render_warp<CAPW, true>, kWarpsPerBlock * 32, smem);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_m, k_render_warp<CAPW, true, true>, kWarpsPerBlock * 32,
+                                                        smem);
     per_sm = per_m > per_sm ? per_m : per_sm;
     if (e != cudaSuccess) return e;
     cached = sms * (per_sm > 0 ? per_sm : 1);
@@ -1603,9 +1610,11 @@ cudaError_t launch_warp(const RenderLaunch& L, cudaStream_t st, const cudaEvent_
   if (e != cudaSuccess) return e;
   if (marks) cudaEventRecord(marks[0], st);
   if (L.flags & kFlagBlueNoise)
-    k_render_warp<CAPW, true><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
+    k_render_warp<CAPW, true, true><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
+  else if (L.counters)
+    k_render_warp<CAPW, false, true><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
   else
-    k_render_warp<CAPW, false><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
+    k_render_warp<CAPW, false, false><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (marks) cudaEventRecord(marks[1], st);
