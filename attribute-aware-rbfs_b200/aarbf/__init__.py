@@ -42,9 +42,9 @@ STORAGE_FP16 = 1        # FP16 positions (relative to 256-particle run origins),
 
 
 def uses_warp_kernel(p) -> bool:
-    """True when a render with these parameters runs the ray-per-warp kernel."""
-    return (int(p.traversal) == TRAVERSAL_AUTO and bool(p.flags & FLAG_MAJORANT_TRACKING)
-            and not p.flags & FLAG_BLUE_NOISE)
+    """True when a render with these parameters runs a ray-per-warp kernel: majorant tracking or
+    stochastic marching (blue-noise mode) with the default traversal."""
+    return int(p.traversal) == TRAVERSAL_AUTO and bool(p.flags & (FLAG_MAJORANT_TRACKING | FLAG_BLUE_NOISE))
 
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "out of memory", 3: "CUDA error",
