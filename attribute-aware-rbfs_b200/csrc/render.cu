@@ -1583,6 +1583,9 @@ cudaError_t warp_grid(int* blocks) {
       e = cudaFuncSetAttribute(k_render_warp<CAPW, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)smem);
     if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_render_warp<CAPW, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem);
+    if (e == cudaSuccess)
       e = cudaFuncSetAttribute(k_render_warp<CAPW, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0, per_sm = 0, per_m = 0;
@@ -1591,7 +1594,7 @@ cudaError_t warp_grid(int* blocks) {
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_warp<CAPW, false, false>, kWarpsPerBlock * 32,
                                                       smem);
     if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_m, k_render_warp<CAPW, true, true>, kWarpsPerBlock * 32,
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_m, k_render_warp<CAPW, true, false>, kWarpsPerBlock * 32,
                                                         smem);
     per_sm = per_m > per_sm ? per_m : per_sm;
     if (e != cudaSuccess) return e;
@@ -1609,8 +1612,10 @@ cudaError_t launch_warp(const RenderLaunch& L, cudaStream_t st, const cudaEvent_
   e = cudaMemsetAsync(L.work_counter, 0, sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
   if (marks) cudaEventRecord(marks[0], st);
-  if (L.flags & kFlagBlueNoise)
+  if ((L.flags & kFlagBlueNoise) && L.counters)
     k_render_warp<CAPW, true, true><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
+  else if (L.flags & kFlagBlueNoise)
+    k_render_warp<CAPW, true, false><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
   else if (L.counters)
     k_render_warp<CAPW, false, true><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
   else
