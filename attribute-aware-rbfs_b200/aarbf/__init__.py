@@ -89,7 +89,7 @@ class Params(ctypes.Structure):
         ("aabb_min", ctypes.c_float * 3), ("aabb_max", ctypes.c_float * 3),
         ("density_gain", ctypes.c_float), ("jitter_x", ctypes.c_float), ("jitter_y", ctypes.c_float),
         ("traversal", ctypes.c_int32), ("density_scale", ctypes.c_float), ("bin_length", ctypes.c_float),
-        ("candidate_cap", ctypes.c_int32), ("stage_bins", ctypes.c_int32),
+        ("candidate_cap", ctypes.c_int32), ("stage_bins", ctypes.c_int32), ("loop_cap", ctypes.c_uint32),
     ]
 
 
@@ -284,6 +284,7 @@ class RenderParams:
     bin_length: float = 0.0
     candidate_cap: int = 0
     stage_bins: int = 0
+    loop_cap: int = 0  # 0: built-in device loop bounds; > 0 lowers them (exercises AARBF_ERR_DEVICE_LIMIT)
 
     def to_c(self) -> Params:
         p = Params()
@@ -299,6 +300,7 @@ class RenderParams:
         p.density_scale, p.bin_length = self.density_scale, self.bin_length
         p.candidate_cap = int(self.candidate_cap)
         p.stage_bins = int(self.stage_bins)
+        p.loop_cap = int(self.loop_cap)
         return p
 
 

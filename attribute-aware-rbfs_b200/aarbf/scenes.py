@@ -183,14 +183,15 @@ def halton_jitter(frame: int):
 
 def native_params(cam, width: int, height: int, rbf_radius: float, unit: float, density_scale: float,
                   dom, spp: int = 1, frame_id: int = 0, traversal: int = 0, marching: bool = False,
-                  majorant: bool = False, bin_length: float = None):
+                  majorant: bool = False, bin_length: float = None, camera_fn=None):
     """Render parameters of the benchmark configurations (native mode: per-particle radii, fp32
     transfer function). Plain form: delta tracking with the global majorant 1/unit, density
     min(density_scale * D * unit, 1) per unit step, from the volume entry. Majorant form: delta
     tracking of extinction density_scale * D with per-bin majorants (bins of bin_length, default
-    4 units)."""
+    4 units). camera_fn(look_from, look_at, look_up, scale, width, height) computes the camera
+    basis (default: the library's aarbf_camera; any function with the same results will do)."""
     from . import camera, FLAG_BLUE_NOISE, FLAG_MAJORANT_TRACKING
-    pos, d00, du, dv = camera(cam[0], cam[1], cam[2], cam[3], width, height)
+    pos, d00, du, dv = (camera_fn or camera)(cam[0], cam[1], cam[2], cam[3], width, height)
     flags = FLAG_VISUALIZE_ATTRIBUTES | FLAG_DENSITY_LINEAR | FLAG_TRACK_FROM_ENTRY | FLAG_SPLAT_PARTICLE_RADIUS
     if marching:
         flags |= FLAG_BLUE_NOISE
@@ -202,3 +203,13 @@ def native_params(cam, width: int, height: int, rbf_radius: float, unit: float, 
                         density_gain=float(np.float32(density_scale) * np.float32(unit)),
                         traversal=traversal, density_scale=float(density_scale),
                         bin_length=float(np.float32(bin_length if bin_length else 4.0 * unit)))
+
+
+def config_small_params(dom, width: int = 512, height: int = 512, spp: int = 1, frame_id: int = 0,
+                        camera_fn=None):
+    """Render parameters of the small configuration (100k particles of config_small): delta
+    tracking with the global majorant 1/unit (the reference's tracker in native mode), step unit
+    0.005 (half the particle radius), density scale 50, orbit camera at distance 2.5 around the
+    unit cube's centre with a 60-degree field of view, 512x512, 1 spp."""
+    return native_params(orbit_camera(distance=2.5, fov_deg=60.0), width, height, 0.01, 0.005, 50.0, dom,
+                         spp=spp, frame_id=frame_id, camera_fn=camera_fn)

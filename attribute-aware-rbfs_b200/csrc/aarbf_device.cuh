@@ -24,6 +24,14 @@ enum : uint32_t {
   kStatusLoopCap = 4u,
 };
 
+// Iteration bound of a device loop: its built-in bound, or the lower one a launch asks for
+// (aarbf_params.loop_cap, which exists to exercise this path). A loop that runs out of
+// iterations ors kStatusLoopCap into the status word, so the caller's aarbf_sync reports
+// AARBF_ERR_DEVICE_LIMIT instead of returning a truncated result as if it were complete.
+__host__ __device__ __forceinline__ int loop_bound(uint32_t requested, int builtin) {
+  return (requested != 0u && requested < (uint32_t)builtin) ? (int)requested : builtin;
+}
+
 // render flags (match AARBF_FLAG_* in include/aarbf.h)
 enum : uint32_t {
   kFlagBlueNoise = 1u << 0,

@@ -5,6 +5,7 @@
 
 #include <array>
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -36,6 +37,32 @@ struct DevBuf {
   T* as() const { return static_cast<T*>(ptr); }
 };
 
+// Launch configuration that belongs to one device: kernel attributes such as the dynamic
+// shared-memory limit are set per device context, and grid sizes follow the device's SM count.
+// Each value is computed once per device, under a lock, by init(device, &value) with that device
+// current; a value of 0 means "not computed yet".
+constexpr int kMaxDevices = 64;
+struct PerDevice {
+  std::mutex mu;
+  int value[kMaxDevices] = {};
+};
+template <class Init>
+cudaError_t per_device(PerDevice& c, int* out, Init&& init) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(c.mu);
+  if (c.value[dev] == 0) {
+    int v = 0;
+    e = init(dev, &v);
+    if (e != cudaSuccess) return e;
+    c.value[dev] = v > 0 ? v : 1;
+  }
+  *out = c.value[dev];
+  return cudaSuccess;
+}
+
 // Everything the tracking / marching / splat kernels read about a built scene.
 struct SceneView {
   const float4* rec0;  // x, y, z, r_eval
@@ -56,6 +83,7 @@ struct SceneView {
   float root_lo[3], root_hi[3];
   float eps;      // absolute slack used by conservative culling tests
   int per_particle_radius;
+  uint32_t loop_cap;  // 0, or a lower iteration bound for every device loop (loop_bound)
   // FP16 storage form (null in the fp32 form): packed records the tracking kernels read
   const uint2* posq;     // FP16 offsets x, y, z from the run origin, FP16 a^3
   const uint2* colq;     // FP16 rgb^2.2 a^3
@@ -121,7 +149,7 @@ cudaError_t launch_collapse(const Node* nodes, uint32_t nleaves, WideNode* wide,
 cudaError_t launch_refit(const float4* rec0, const float* rgeom, uint64_t n, uint32_t ppl,
                          uint32_t nleaves, Node* nodes, Node* nodes_ref, const uint32_t* leaf_parent,
                          uint32_t* counters, float* leaf_box, float* leaf_eff, float* root_box,
-                         cudaStream_t st);
+                         uint32_t* status, cudaStream_t st);
 // the tracking kernels, built for the fp32 records (r32) and the FP16 storage form (r16)
 struct BatchArgs;
 #define AARBF_RENDER_DECLS                                                                      \
@@ -150,7 +178,7 @@ inline cudaError_t render_warp_stack_words(size_t* words) {
 // slabs: the splat slab starts (nslabs entries, the last beyond every ray's exit) for the
 // ray-per-warp splat kernel; NULL selects the thread-per-pixel kernel
 cudaError_t launch_splat(const RenderLaunch& L, cudaStream_t st, const float* slabs = nullptr, int nslabs = 0);
-size_t splat_stack_words();
+cudaError_t splat_stack_words(size_t* words);
 
 // several scenes in one persistent launch of the ray-per-warp kernel (render.cu)
 struct BatchArgs {
@@ -190,7 +218,7 @@ struct DiffArgs {
   bool backward;
 };
 cudaError_t launch_diff(const DiffArgs& A, cudaStream_t st);
-size_t diff_stack_words();
+cudaError_t diff_stack_words(size_t* words);
 cudaError_t launch_diff_finish(const float4* xyzw, const uint32_t* perm, uint64_t n, const float4* tf, int nc,
                                float attr_scale, const float* g_pos, const float* g_rad, const float* g_w,
                                float* out_pos, float* out_rad, float* out_attr, float* out_tf, cudaStream_t st);

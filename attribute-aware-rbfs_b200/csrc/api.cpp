@@ -129,7 +129,8 @@ aarbf_status run_refit(aarbf_ctx* ctx, cudaStream_t st) {
        "fp16 weights");
   CK(launch_refit(ctx->rec0.as<float4>(), ctx->rgeom.as<float>(), n, ctx->ppl, ctx->nleaves, ctx->nodes.as<Node>(),
                   ctx->nodes_ref.as<Node>(), ctx->leaf_parent.as<uint32_t>(), ctx->counters.as<uint32_t>(),
-                  ctx->leaf_box.as<float>(), ctx->leaf_eff.as<float>(), ctx->root_box.as<float>(), st),
+                  ctx->leaf_box.as<float>(), ctx->leaf_eff.as<float>(), ctx->root_box.as<float>(),
+                  ctx->status.as<uint32_t>(), st),
      "refit");
   if (ctx->nleaves > 1) {
     const size_t wb = sizeof(WideNode) * (size_t)(ctx->nleaves - 1);
@@ -234,6 +235,7 @@ aarbf_status fill_launch(aarbf_ctx* ctx, const aarbf_params* p, int w, int h, fl
   L.accum = reinterpret_cast<float4*>(accum);
   L.image = reinterpret_cast<float4*>(image);
   L.status = ctx->status.as<uint32_t>();
+  L.s.loop_cap = p->loop_cap;
   L.traversal = p->traversal;
   L.splat_rmax = (p->flags & kFlagSplatParticleRadius) ? ctx->max_radius : p->rbf_radius;
   L.density_scale = p->density_scale;
@@ -255,6 +257,13 @@ aarbf_status fill_launch(aarbf_ctx* ctx, const aarbf_params* p, int w, int h, fl
     }
   }
   if (!(p->unit > 0.0f)) return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "unit must be > 0");
+  {
+    // the persistent kernels count work items (one sample of one pixel, pixels padded to 8 x 4
+    // tiles) in 32 bits, and every resident warp or thread takes one item past the end
+    const uint64_t items = (uint64_t)((w + 7) / 8) * (uint64_t)((h + 3) / 4) * 32u * L.spp;
+    if (items > 0xfff00000ull)
+      return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "width x height x spp exceeds the 32-bit work-item count");
+  }
   if ((p->flags & kFlagMajorantTracking) && !(p->bin_length > 0.0f && p->density_scale >= 0.0f))
     return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "majorant tracking needs bin_length > 0, density_scale >= 0");
   if (!ctx->work.ptr) CK(ctx->work.reserve(256), "work counter");
@@ -867,6 +876,7 @@ static aarbf_status diff_setup(aarbf_ctx* ctx, const aarbf_params* views, int nv
   CK(cudaStreamSynchronize(st), "views upload");
   memset(&A, 0, sizeof(A));
   fill_scene_view(ctx, views[0].cam_pos, A.s);
+  A.s.loop_cap = views[0].loop_cap;
   for (int v = 1; v < nviews; ++v) A.s.eps = std::fmax(A.s.eps, scene_eps(ctx, views[v].cam_pos));
   A.views = ctx->diff_views.ptr;
   A.nviews = nviews;
@@ -875,7 +885,11 @@ static aarbf_status diff_setup(aarbf_ctx* ctx, const aarbf_params* views, int nv
   if (!ctx->work.ptr) CK(ctx->work.reserve(256), "work counter");
   A.work_counter = ctx->work.as<uint32_t>();
   A.status = ctx->status.as<uint32_t>();
-  CK(ctx->warp_stacks.reserve(4 * diff_stack_words()), "warp stacks");
+  {
+    size_t words = 0;
+    CK(diff_stack_words(&words), "differentiable kernel setup");
+    CK(ctx->warp_stacks.reserve(4 * words), "warp stacks");
+  }
   A.warp_stacks = ctx->warp_stacks.as<uint32_t>();
   ctx->diff_samples = (size_t)nviews * (size_t)w * (size_t)h * spp0;
   ctx->diff_spp = spp0;
@@ -992,7 +1006,11 @@ aarbf_status aarbf_render_splat(aarbf_ctx* ctx, const aarbf_params* p, int w, in
   }
   if (!ctx->work.ptr) CK(ctx->work.reserve(256), "work counter");
   L.work_counter = ctx->work.as<uint32_t>();
-  CK(ctx->warp_stacks.reserve(4 * splat_stack_words()), "warp stacks");
+  {
+    size_t words = 0;
+    CK(splat_stack_words(&words), "splat kernel setup");
+    CK(ctx->warp_stacks.reserve(4 * words), "warp stacks");
+  }
   L.warp_stacks = ctx->warp_stacks.as<uint32_t>();
   CK(launch_splat(L, st, ctx->splat_slabs.as<float>(), ctx->splat_nslabs), "splat launch");
   return AARBF_OK;

@@ -192,7 +192,12 @@ __device__ float3 diff_sample(const DiffLaunch& L, const DiffView& V, int px, in
   float tau_c = 0.0f, gp_c = 0.0f;              // carries: optical depth, g' of the last step with D > 0
   float3 P_c = make_float3(0.0f, 0.0f, 0.0f);   // backward: prefix of B
   int k0 = 0, m = 32;
-  for (int guard = 0; guard < (1 << 22); ++guard) {
+  const int cap = loop_bound(s.loop_cap, 1 << 22);
+  for (int guard = 0;; ++guard) {
+    if (guard == cap) {  // the loop bound ran out: report the truncated ray
+      if (lane == 0) atomicOr(L.status, kStatusLoopCap);
+      break;
+    }
     const float ta = t0 + (float)(k0 + 1) * unit;
     if (!(ta < texit)) break;
     const float tb = fminf(t0 + (float)(k0 + m) * unit, texit);
@@ -441,27 +446,32 @@ __global__ void k_diff_finish(const float4* __restrict__ xyzw, const uint32_t* _
     if (sh_tf[j] != 0.0f) atomicAdd(out_tf + j, sh_tf[j]);
 }
 
-int diff_grid_blocks() {
-  static int cached = 0;
-  if (!cached) {
-    const size_t smem = sizeof(DiffBuf) * kDiffWarps;
-    cudaFuncSetAttribute(k_diff<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_diff<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int dev = 0, sms = 0, a = 0, b = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_diff<false>, kDiffWarps * 32, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_diff<true>, kDiffWarps * 32, smem);
-    cached = sms * max(1, min(a, b));
-  }
-  return cached;
+// grid of the differentiable kernels on the current device (sets their shared-memory limit there)
+cudaError_t diff_grid_blocks(int* blocks) {
+  static PerDevice cache;
+  return per_device(cache, blocks, [](int dev, int* v) {
+    const int smem = (int)(sizeof(DiffBuf) * kDiffWarps);
+    cudaError_t e = cudaFuncSetAttribute(k_diff<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_diff<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int sms = 0, a = 0, b = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_diff<false>, kDiffWarps * 32, smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_diff<true>, kDiffWarps * 32, smem);
+    *v = sms * max(1, min(a, b));
+    return e;
+  });
 }
 
 static_assert(sizeof(DiffView) == sizeof(float) * 22, "DiffView layout");
 
 }  // namespace
 
-size_t diff_stack_words() { return (size_t)diff_grid_blocks() * kDiffWarps * kWarpStack; }
+cudaError_t diff_stack_words(size_t* words) {
+  int blocks = 0;
+  cudaError_t e = diff_grid_blocks(&blocks);
+  *words = (size_t)blocks * kDiffWarps * kWarpStack;
+  return e;
+}
 
 cudaError_t launch_diff(const DiffArgs& A, cudaStream_t st) {
   if (A.width <= 0 || A.height <= 0 || A.nviews <= 0) return cudaSuccess;
@@ -480,7 +490,9 @@ cudaError_t launch_diff(const DiffArgs& A, cudaStream_t st) {
   L.work_counter = A.work_counter;
   L.status = A.status;
   L.warp_stacks = A.warp_stacks;
-  const int blocks = diff_grid_blocks();
+  int blocks = 0;
+  cudaError_t eg = diff_grid_blocks(&blocks);
+  if (eg != cudaSuccess) return eg;
   cudaError_t e = cudaMemsetAsync(A.work_counter, 0, sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
   const size_t smem = sizeof(DiffBuf) * kDiffWarps;

@@ -119,7 +119,7 @@ __device__ __forceinline__ void nan_if_empty(float* lo, float* hi) {
 __global__ void k_refit(const float4* __restrict__ rec0, const float* __restrict__ rgeom, uint64_t n,
                         uint32_t ppl, uint32_t nleaves, Node* nodes, Node* nodes_ref,
                         const uint32_t* __restrict__ leaf_parent, uint32_t* counters, float* __restrict__ leaf_box,
-                        float* __restrict__ leaf_eff, float* __restrict__ root_box) {
+                        float* __restrict__ leaf_eff, float* __restrict__ root_box, uint32_t* status) {
   uint64_t l = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (l >= nleaves) return;
   const float inf = __int_as_float(0x7f800000);
@@ -183,6 +183,9 @@ __global__ void k_refit(const float4* __restrict__ rec0, const float* __restrict
     child = parent;
     parent = up;
   }
+  // a Karras tree over 48-bit keys with index tie-breaks is at most 80 levels deep, so the
+  // climb cannot run out of its 256 iterations on a well-formed tree; report it if it does
+  atomicOr(status, kStatusLoopCap);
 }
 
 // largest non-negative bounds radius (max over the float bits, which order like the values)
@@ -278,14 +281,14 @@ cudaError_t launch_karras(const uint64_t* sorted_keys, uint64_t n, uint32_t ppl,
 
 cudaError_t launch_refit(const float4* rec0, const float* rgeom, uint64_t n, uint32_t ppl, uint32_t nleaves,
                          Node* nodes, Node* nodes_ref, const uint32_t* leaf_parent, uint32_t* counters,
-                         float* leaf_box, float* leaf_eff, float* root_box, cudaStream_t st) {
+                         float* leaf_box, float* leaf_eff, float* root_box, uint32_t* status, cudaStream_t st) {
   if (!nleaves) return cudaSuccess;
   if (nleaves > 1) {
     cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(uint32_t) * (nleaves - 1), st);
     if (e != cudaSuccess) return e;
   }
   k_refit<<<blocks_for(nleaves, 256), 256, 0, st>>>(rec0, rgeom, n, ppl, nleaves, nodes, nodes_ref, leaf_parent,
-                                                   counters, leaf_box, leaf_eff, root_box);
+                                                   counters, leaf_box, leaf_eff, root_box, status);
   return cudaGetLastError();
 }
 

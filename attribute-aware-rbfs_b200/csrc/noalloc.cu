@@ -17,7 +17,12 @@
 //    work overlaps in time (different streams, or host threads) race on it and must be ordered
 //    by the caller;
 //  - the first call on a device resolves the array's device address (cudaGetSymbolAddress, with
-//    that device current) and caches it; make that first call before any stream capture.
+//    that device current) and caches it; make that first call before any stream capture. The
+//    cached address belongs to the device's primary context: it must not outlive a
+//    cudaDeviceReset of that device;
+//  - xyzw, keys and perm must be device (or managed) memory: host pointers are refused with
+//    AARBF_ERR_INVALID_ARGUMENT before any GPU work (cudaPointerGetAttributes, which allocates
+//    nothing).
 #include <cstring>
 #include <mutex>
 
@@ -42,9 +47,18 @@ constexpr size_t kScratchBytes = kOffFlag + 256;
 // device address comes from cudaGetSymbolAddress below.
 __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 unsigned char* g_scratch_ptr[kMaxDevices] = {};
+
+// true for memory a kernel on the current device may read and write
+bool device_accessible(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // clear the (non-sticky) error the query recorded
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
 
 }  // namespace
 
@@ -57,6 +71,8 @@ extern "C" aarbf_status aarbf_hilbert_sort_noalloc(const float* xyzw, uint64_t n
   if (n > kNoallocMaxParticles) return AARBF_ERR_INVALID_ARGUMENT;
   if (n && (!xyzw || !dom || !keys || !perm)) return AARBF_ERR_INVALID_ARGUMENT;
   if (!n) return AARBF_OK;
+  if (!device_accessible(xyzw) || !device_accessible(keys) || !device_accessible(perm))
+    return AARBF_ERR_INVALID_ARGUMENT;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return AARBF_ERR_CUDA;
   unsigned char* base;

@@ -572,7 +572,9 @@ __device__ void track_majorant(const RenderLaunch& L, Tracker& tr, const Ray& ra
   int seg_end = 0;   // bins below seg_end are covered by the staged candidates
   int nb = L.stage_bins;  // bins per staging
   bool direct = false;
-  for (int guard = 0; guard < (1 << 26); ++guard) {
+  const int cap = loop_bound(L.s.loop_cap, 1 << 26);
+  int guard = 0;
+  for (; guard < cap; ++guard) {
     float b0 = t0 + (float)k * Lb;
     float b1 = t0 + (float)(k + 1) * Lb;
     if (!(b0 < ray.tmax) || !(b1 > b0)) break;
@@ -683,6 +685,7 @@ __device__ void track_majorant(const RenderLaunch& L, Tracker& tr, const Ray& ra
     k += 1;
     t = b1;
   }
+  if (guard == cap) atomicOr(L.status, kStatusLoopCap);
   tr.t = t;
 }
 
@@ -1093,7 +1096,9 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
   int seg_end = 0;
   int nb = L.stage_bins;
   bool direct = false;
-  for (int guard = 0; guard < (1 << 26); ++guard) {
+  const int cap = loop_bound(L.s.loop_cap, 1 << 26);
+  int guard = 0;
+  for (; guard < cap; ++guard) {
     float b0 = t0 + (float)k * Lb;
     float b1 = t0 + (float)(k + 1) * Lb;
     if (!(b0 < ray.tmax) || !(b1 > b0)) break;
@@ -1193,6 +1198,7 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
     k += 1;
     t = b1;
   }
+  if (guard == cap && (threadIdx.x & 31u) == 0) atomicOr(L.status, kStatusLoopCap);
   tr.t = t;
 }
 
@@ -1267,7 +1273,8 @@ __device__ __forceinline__ void track_march_warp_body(const RenderLaunch& L, Tra
   const float rhs = -dlog(1.0f - tr.random * 0.99f);
   const float3 inv = make_float3(1.0f / ray.d.x, 1.0f / ray.d.y, 1.0f / ray.d.z);
   int m = 32;
-  for (int guard = 0; guard < (1 << 22); ++guard) {
+  const int cap = loop_bound(s.loop_cap, 1 << 22);
+  for (int guard = 0; guard < cap; ++guard) {
     if (tr.i >= kMaxDepth) return;
     // the chunk's step positions: the running sum, lane j keeps step j
     float tj = 0.0f, t = tr.t;
@@ -1362,6 +1369,7 @@ __device__ __forceinline__ void track_march_warp_body(const RenderLaunch& L, Tra
     tr.albedo.w = alpha;
     if (m < 32) m <<= 1;
   }
+  if (lane == 0) atomicOr(L.status, kStatusLoopCap);  // the loop bound ran out
 }
 
 template <int CAPW>
@@ -1541,18 +1549,18 @@ __global__ void k_accumulate_batched(const RenderLaunch* __restrict__ Ls, const 
 template <int CAP>
 cudaError_t launch_cap(const RenderLaunch& L, cudaStream_t st, const cudaEvent_t* marks) {
   const size_t smem = (sizeof(uint32_t) + 2 * sizeof(float)) * CAP * kBlock;
-  static int blocks = 0;
-  if (!blocks) {
-    cudaError_t e = cudaFuncSetAttribute(k_render<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render<CAP>, kBlock, smem);
-    if (e != cudaSuccess) return e;
-    blocks = sms * (per_sm > 0 ? per_sm : 1);
-  }
-  cudaError_t e = cudaMemsetAsync(L.work_counter, 0, sizeof(uint32_t), st);
+  static PerDevice cache;
+  int blocks = 0;
+  cudaError_t e = per_device(cache, &blocks, [&](int dev, int* v) {
+    cudaError_t r = cudaFuncSetAttribute(k_render<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int sms = 0, per_sm = 0;
+    if (r == cudaSuccess) r = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (r == cudaSuccess) r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render<CAP>, kBlock, smem);
+    *v = sms * (per_sm > 0 ? per_sm : 1);
+    return r;
+  });
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(L.work_counter, 0, sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
   uint64_t items = (uint64_t)((L.width + 7) / 8) * (uint64_t)((L.height + 3) / 4) * 32u * (L.spp ? L.spp : 1u);
   int grid = (int)((items + kBlock - 1) / kBlock);
@@ -1572,36 +1580,33 @@ cudaError_t launch_cap(const RenderLaunch& L, cudaStream_t st, const cudaEvent_t
 
 namespace {
 
+// Grid of the ray-per-warp kernels on the current device: the occupancy of the timed instances
+// (the count-mode instances have larger frames and run oversubscribed on the same grid; work comes
+// from an atomic counter, so that is still correct). Also sets the shared-memory limit of every
+// instance, including the batched kernel, on this device.
 template <int CAPW>
 cudaError_t warp_grid(int* blocks) {
-  static int cached = 0;
-  if (!cached) {
-    const size_t smem = sizeof(WarpBuf<CAPW>) * kWarpsPerBlock;
-    cudaError_t e =
-        cudaFuncSetAttribute(k_render_warp<CAPW, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  static PerDevice cache;
+  return per_device(cache, blocks, [](int dev, int* v) {
+    const int smem = (int)(sizeof(WarpBuf<CAPW>) * kWarpsPerBlock);
+    const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaError_t e = cudaFuncSetAttribute(k_render_warp<CAPW, false, false>, attr, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_render_warp<CAPW, false, true>, attr, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_render_warp<CAPW, true, false>, attr, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_render_warp<CAPW, true, true>, attr, smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_render_warp_batched<CAPW>, attr, smem);
+    int sms = 0, per_sm = 0, per_m = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_render_warp<CAPW, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_warp<CAPW, false, false>,
+                                                        kWarpsPerBlock * 32, smem);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_render_warp<CAPW, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_render_warp<CAPW, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    int dev = 0, sms = 0, per_sm = 0, per_m = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_warp<CAPW, false, false>, kWarpsPerBlock * 32,
-                                                      smem);
-    if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_m, k_render_warp<CAPW, true, false>, kWarpsPerBlock * 32,
-                                                        smem);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_m, k_render_warp<CAPW, true, false>,
+                                                        kWarpsPerBlock * 32, smem);
     per_sm = per_m > per_sm ? per_m : per_sm;
-    if (e != cudaSuccess) return e;
-    cached = sms * (per_sm > 0 ? per_sm : 1);
-  }
-  *blocks = cached;
-  return cudaSuccess;
+    *v = sms * (per_sm > 0 ? per_sm : 1);
+    return e;
+  });
 }
 
 template <int CAPW>
@@ -1652,13 +1657,6 @@ cudaError_t launch_warp_batched(const BatchArgs& B, cudaStream_t st) {
   int blocks = 0;
   cudaError_t e = warp_grid<CAPW>(&blocks);
   if (e != cudaSuccess) return e;
-  static bool configured = false;
-  if (!configured) {
-    e = cudaFuncSetAttribute(k_render_warp_batched<CAPW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(sizeof(WarpBuf<CAPW>) * kWarpsPerBlock));
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
   e = cudaMemsetAsync(B.work_counter, 0, sizeof(unsigned long long), st);
   if (e != cudaSuccess) return e;
   k_render_warp_batched<CAPW><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(

@@ -140,9 +140,13 @@ __global__ void __launch_bounds__(kBlock) k_splat(const RenderLaunch L, float pa
     const float atten = dexp(-L.unit * (float)(kKeep / 8));
     float tslab = 0.0f;
     int run = 16;  // slabs staged per traversal
+    const int cap = loop_bound(L.s.loop_cap, 1 << 24);
     int guard = 0;
-    while (tslab < texit && guard < (1 << 24)) {
-      ++guard;
+    while (tslab < texit) {
+      if (guard++ == cap) {  // the loop bound ran out: report the truncated pixel
+        atomicOr(L.status, kStatusLoopCap);
+        break;
+      }
       if (res.w > 0.99f) break;
       // skip slabs that end before the entry point
       float tmax0 = fminf(texit, tslab + spacing);
@@ -327,7 +331,12 @@ __global__ void __launch_bounds__(kSplatWarps * 32) k_splat_warp(const __grid_co
       // first slab whose end lies beyond the entry point
       int k = first_above(A.slabs, 1, A.nslabs, tenter) - 1;
       int run = 64;
-      for (int guard = 0; guard < (1 << 22) && k + 1 < A.nslabs; ++guard) {
+      const int cap = loop_bound(L.s.loop_cap, 1 << 22);
+      for (int guard = 0; k + 1 < A.nslabs; ++guard) {
+        if (guard == cap) {  // the loop bound ran out: report the truncated pixel
+          if (lane == 0) atomicOr(L.status, kStatusLoopCap);
+          break;
+        }
         const float ts = __ldg(A.slabs + k);
         if (!(ts < texit) || res.w > 0.99f) break;
         const int kend = min(k + run, A.nslabs - 1);
@@ -446,18 +455,18 @@ __global__ void __launch_bounds__(kSplatWarps * 32) k_splat_warp(const __grid_co
   }
 }
 
-int splat_grid_blocks() {
-  static int cached = 0;
-  if (!cached) {
-    const size_t smem = sizeof(SplatBuf) * kSplatWarps;
-    cudaFuncSetAttribute(k_splat_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int dev = 0, sms = 0, per = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_splat_warp, kSplatWarps * 32, smem);
-    cached = sms * (per > 0 ? per : 1);
-  }
-  return cached;
+// grid of the ray-per-warp splat kernel on the current device (sets its shared-memory limit there)
+cudaError_t splat_grid_blocks(int* blocks) {
+  static PerDevice cache;
+  return per_device(cache, blocks, [](int dev, int* v) {
+    const int smem = (int)(sizeof(SplatBuf) * kSplatWarps);
+    cudaError_t e = cudaFuncSetAttribute(k_splat_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int sms = 0, per = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_splat_warp, kSplatWarps * 32, smem);
+    *v = sms * (per > 0 ? per : 1);
+    return e;
+  });
 }
 
 }  // namespace
@@ -480,7 +489,10 @@ cudaError_t launch_splat(const RenderLaunch& L, cudaStream_t st, const float* sl
     A.warp_stacks = L.warp_stacks;
     cudaError_t e = cudaMemsetAsync(L.work_counter, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
-    k_splat_warp<<<splat_grid_blocks(), kSplatWarps * 32, sizeof(SplatBuf) * kSplatWarps, st>>>(L, A);
+    int blocks = 0;
+    e = splat_grid_blocks(&blocks);
+    if (e != cudaSuccess) return e;
+    k_splat_warp<<<blocks, kSplatWarps * 32, sizeof(SplatBuf) * kSplatWarps, st>>>(L, A);
     return cudaGetLastError();
   }
   dim3 grid((L.width + 15) / 16, (L.height + 7) / 8);
@@ -488,6 +500,11 @@ cudaError_t launch_splat(const RenderLaunch& L, cudaStream_t st, const float* sl
   return cudaGetLastError();
 }
 
-size_t splat_stack_words() { return (size_t)splat_grid_blocks() * kSplatWarps * kWarpStack; }
+cudaError_t splat_stack_words(size_t* words) {
+  int blocks = 0;
+  cudaError_t e = splat_grid_blocks(&blocks);
+  *words = (size_t)blocks * kSplatWarps * kWarpStack;
+  return e;
+}
 
 }  // namespace aarbf

@@ -82,7 +82,12 @@ __device__ bool warp_traverse_wide(const SceneView& s, const WideNode* wide, uin
   if (lane == 0) stk[0] = s.root;
   int sp = 1;
   __syncwarp();
-  for (int guard = 0; sp > 0 && guard < (1 << 24); ++guard) {
+  const int cap = loop_bound(s.loop_cap, 1 << 24);
+  for (int guard = 0; sp > 0; ++guard) {
+    if (guard == cap) {  // truncated traversal: report it
+      if (lane == 0) atomicOr(status, kStatusLoopCap);
+      return false;
+    }
     constexpr int kPer = 32 / kBvhWidth;
     const int take = sp < kPer ? sp : kPer;
     const int base = sp - take;

@@ -14,11 +14,16 @@ value      : rays of all ranks / max-over-ranks device time of the K timed steps
 e2e        : the same metric through the public C ABI with host buffers: per step the particle
              upload (pinned host -> device), the build (Hilbert sort + LBVH), the render and the
              image read-back are inside the timed region
-roofline   : algorithmic bytes of one render launch (20 B per particle whose sphere meets a
-             traversed ray segment + 64 B per BVH node visit + 48 B per pixel of framebuffer
-             traffic) / measured launch time, against the measured HBM copy bandwidth
+roofline   : algorithmic bytes of one render launch / measured launch time, against the measured
+             HBM copy bandwidth. Algorithmic bytes: 20 B per particle whose sphere meets a
+             traversed ray segment (16 B record + 4 B radius) + 32 B per BVH node visit of those
+             segment queries + 48 B per sample of framebuffer traffic (accum read and write, image
+             write: spp x W x H x 48 B). The same figure with this library's own 64-byte nodes and
+             per-pixel framebuffer traffic is reported beside it.
 cpu_baseline: the oracle (C restatement of the reference's device code, OpenMP over pixels) on a
-             bounded, evenly spread sample of the same frame's pixels, on this host's cores
+             bounded, evenly spread sample of the same frame's pixels, on this host's cores; the
+             GPU renders the same frame at the same spp and its pixels in the sampled tiles are
+             compared bit for bit with the oracle's ("parity")
 Multi-GPU: replicas (each rank renders its own frames of the replicated scene; weak scaling).
 """
 import argparse
@@ -181,13 +186,13 @@ def domain_of(xyzw):
     return d
 
 
-def params_for(args, dom, rmax, frame_id=0, estimator=None, spp=None):
+def params_for(args, dom, rmax, frame_id=0, estimator=None, spp=None, camera_fn=None):
     from aarbf import scenes
     est = estimator or args.estimator
     rp = scenes.native_params(scenes.orbit_camera(), args.width, args.height, rmax, args.unit,
                               args.density_scale, dom, spp=spp or args.spp, frame_id=frame_id,
                               traversal=args.traversal, majorant=(est == "majorant"),
-                              bin_length=args.bin * args.unit)
+                              bin_length=args.bin * args.unit, camera_fn=camera_fn)
     rp.candidate_cap = args.cap if est == "majorant" else 0
     return rp
 
@@ -197,9 +202,10 @@ def cpu_scene(args, sc, tf, dom, rbf_radius):
     return orc.build_scene(sc.xyzw, sc.radii, dom, args.ppl, rbf_radius, tf, args.alpha_floor)[0]
 
 
-def cpu_sample(args, scene, rp, target_s, threads):
-    """Render an evenly spread sample of the frame's pixels with the oracle; returns
-    (Mrays/s, rays, seconds, description)."""
+def cpu_sample(args, scene, rp, target_s, threads, out=None):
+    """Render an evenly spread sample of the frame's pixels with the oracle at 1 spp; returns
+    (Mrays/s, rays, seconds, description). out (optional dict) receives the oracle's image and
+    the sampled tiles (x0, y0, size) of the last, timed pass."""
     import oracle.oracle as orc
     p = orc.params_from(rp)
     p.spp = 1
@@ -211,22 +217,38 @@ def cpu_sample(args, scene, rp, target_s, threads):
     def run(ntiles_side):
         xs = np.linspace(0, W - tile, ntiles_side).astype(int)
         ys = np.linspace(0, H - tile, ntiles_side).astype(int)
+        accum[:] = 0.0
         t0 = time.perf_counter()
         for y in ys:
             for x in xs:
                 scene.render(p, W, H, accum=accum, threads=threads, image=image,
                              region=(int(x), int(x) + tile, int(y), int(y) + tile))
         dt = time.perf_counter() - t0
-        return len(xs) * len(ys) * tile * tile, dt
+        return len(xs) * len(ys) * tile * tile, dt, [(int(x), int(y), tile) for y in ys for x in xs]
 
-    rays, dt = run(4)
+    rays, dt, tiles = run(4)
     side = 4
     while dt < target_s * 0.4 and side < 64:
         side = min(64, int(side * max(1.5, (target_s / max(dt, 1e-3)) ** 0.5)))
-        rays, dt = run(side)
+        rays, dt, tiles = run(side)
     desc = (f"{side}x{side} tiles of {tile}x{tile} pixels spread evenly over the {W}x{H} frame, 1 spp "
             f"({rays} rays) of the same scene, camera and estimator")
+    if out is not None:
+        out["image"], out["tiles"] = image, tiles
     return rays / dt / 1e6, rays, dt, desc
+
+
+def tile_parity(gpu_image, cpu):
+    """Bit-for-bit comparison of the GPU frame with the oracle on the oracle's sampled tiles."""
+    g = np.ascontiguousarray(gpu_image).view(np.uint32)
+    o = np.ascontiguousarray(cpu["image"]).view(np.uint32)
+    pixels = mism = 0
+    for x, y, t in cpu["tiles"]:
+        a, b = g[y:y + t, x:x + t], o[y:y + t, x:x + t]
+        pixels += t * t
+        mism += int((a != b).any(axis=-1).sum())
+    return {"pixels": pixels, "mismatches": mism, "spp": 1,
+            "compared": "every float of the image in the CPU baseline's tiles, GPU frame vs oracle, bit for bit"}
 
 
 def run_reference(args):
@@ -234,10 +256,11 @@ def run_reference(args):
     rank, _, world = dist_env()
     if world > 1 and rank != 0:
         return
+    import oracle.oracle as orc
     threads = os.cpu_count() or 1
     sc, tf = make_scene(args)
     dom = domain_of(sc.xyzw)
-    rp = params_for(args, dom, float(sc.radii.max()))
+    rp = params_for(args, dom, float(sc.radii.max()), camera_fn=orc.camera)  # no product library here
     scene = cpu_scene(args, sc, tf, dom, rp.rbf_radius)
     vals = []
     for k in range(args.warmup + args.steps):
@@ -754,7 +777,10 @@ def main():
     rp = params_for(args, dom, rmax, frame_id=0)
     counts = ctx.render_count(rp, W, H, accum, image, stream=sp)
     parts, visits = counts["segment_particles"], counts["segment_nodes"]
-    alg_bytes = 20 * parts + 64 * visits + 48 * W * H
+    # 20 B per particle on a traversed segment, 32 B per node visit, 48 B per sample
+    alg_bytes = 20 * parts + 32 * visits + 48 * W * H * S
+    # the same with this library's 64-byte nodes and per-pixel framebuffer traffic
+    alg_bytes_own = 20 * parts + 64 * visits + 48 * W * H
     launch_s = render_ms / 1e3 / max(timed_renders, 1)
     achieved = alg_bytes / launch_s / 1e9
     peak, peak_kind = measured_peak()
@@ -811,19 +837,28 @@ def main():
 
     cpu = None
     rmse = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         scene = cpu_scene(args, sc, tf, dom, rp.rbf_radius)
-        v, r_cpu, dt, desc = cpu_sample(args, scene, rp, args.cpu_seconds, threads)
+        sampled = {}
+        v, r_cpu, dt, desc = cpu_sample(args, scene, rp, args.cpu_seconds, threads, out=sampled)
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc,
                "seconds": round(dt, 2)}
+        # the GPU's render of the same frame at 1 spp, compared with the oracle on the sampled tiles
+        rp1 = params_for(args, dom, rmax, frame_id=0, spp=1)
+        accum.zero_()
+        ctx.render(rp1, W, H, accum, image, stream=sp)
+        ctx.sync(sp)
+        parity = tile_parity(image.cpu().numpy(), sampled)
         if args.rmse_crop > 0 and args.rmse_ref_spp > 0:
             rmse = rmse_study(ctx, args, scene, dom, rmax, threads, stream)
             plain_v = plain["value"] if plain else None
             ms = rmse["rmse"]
             if plain_v and ms["majorant_gpu"] > 0:
                 rmse["speedup_vs_plain_gpu"] = (value / plain_v) * (ms["plain_gpu"] / ms["majorant_gpu"]) ** 2
-            rmse["speedup_vs_cpu"] = value / v  # the CPU port's images are bit-identical: equal RMSE
+            if parity and parity["mismatches"] == 0:
+                rmse["speedup_vs_cpu"] = value / v  # same images (parity record): equal RMSE
 
     if rank == 0:
         line = {
@@ -834,11 +869,18 @@ def main():
             "config": config_dict(args),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profiled_traffic(args), "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": alg_bytes, "particles_on_segments": parts,
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "bytes_rule": "20 B x particles on traversed segments + 32 B x node visits + "
+                                       "48 B x spp x W x H",
+                         "achieved_own_layout": alg_bytes_own / launch_s / 1e9,
+                         "algorithmic_bytes_own_layout": alg_bytes_own,
+                         "own_layout_rule": "20 B x particles + 64 B x node visits (this library's node "
+                                            "size) + 48 B x W x H",
+                         "particles_on_segments": parts,
                          "node_visits": visits, "kernel": "k_render_warp" if aarbf.uses_warp_kernel(rp)
                          else "k_render", "kernel_ms": launch_s * 1e3,
                          "accumulate_ms": accumulate_ms / max(timed_renders, 1), "kernel_counters": counts},
-            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": 2 * timed_renders,
+            "cpu_baseline": cpu, "parity": parity, "e2e": e2e, "clocks": clk, "gpu_launches": 2 * timed_renders,
             "build_ms": build_s * 1e3, "build": build, "plain_estimator": plain, "variants": variants, "equal_rmse": rmse,
             "differentiable": diff, "batched": batched, "precision": precision, "series": series,
         }

@@ -93,6 +93,13 @@ typedef struct aarbf_params {
   int32_t stage_bins;       /* majorant tracking: bins staged by the first traversal of a ray
                                (1..64; 0 = 4 for the warp kernel, 16 per thread; later stagings
                                double up to 64); tuning only */
+  uint32_t loop_cap;        /* 0 = the built-in iteration bounds of the device loops (the
+                               reference's MAX_DEPTH step budget is not one of them). A positive
+                               value lowers every bound to it, so the status path can be
+                               exercised: a loop that runs out of iterations leaves its pixel
+                               incomplete and makes the next aarbf_sync return
+                               AARBF_ERR_DEVICE_LIMIT (the reference caps its loops silently at
+                               MAX_DEPTH, sharedCode.h:27). */
 } aarbf_params;
 
 /* ---- context -------------------------------------------------------------------------- */
@@ -291,7 +298,10 @@ aarbf_status aarbf_series_save(const char *path, const float *const *frames, con
  * until the process exits (about 12.5 MiB), so n is limited to AARBF_NOALLOC_MAX_PARTICLES;
  * larger n returns AARBF_ERR_INVALID_ARGUMENT. All calls share that array: calls whose GPU work
  * overlaps (other streams, other host threads) race and must be ordered by the caller. The first
- * call on a device looks up the array's address; make it before any stream capture. The call
+ * call on a device looks up the array's address; make it before any stream capture. That address
+ * is cached for the life of the device's primary context: do not keep calling across a
+ * cudaDeviceReset. Host pointers for xyzw, keys or perm are refused with
+ * AARBF_ERR_INVALID_ARGUMENT before any GPU work. The call
  * synchronises `stream` once (to read the tie flag), like aarbf_build. */
 #define AARBF_NOALLOC_MAX_PARTICLES (1u << 20)
 aarbf_status aarbf_hilbert_sort_noalloc(const float *xyzw, uint64_t n, const float *dom,

@@ -7,7 +7,7 @@
  * round-to-nearest operation, fmaf() is written out where a fused step is meant.
  *
  * Parity model fixed here (the reference leaves these to the un-vendored GPRT runtime
- * or to hardware; each choice is documented in DESIGN.md):
+ * or to hardware; the CUDA path makes the same choices):
  *   - exp/log/pow: Cody-Waite reduction + Taylor / atanh series (orc_expf/orc_logf);
  *   - textures: linear filter at texel centres, clamp-to-edge, sRGB decode of R,G,B;
  *   - any-hit accumulation: exact fixed-point sums (2^-40 units), order independent;

@@ -1,6 +1,7 @@
 """Batched rendering (aarbf_batch_create / aarbf_batch_render): several scenes of different
 sizes, resolutions and spp in one persistent launch give the same bits as one aarbf_render per
-scene, also when the launch is replayed from a CUDA graph."""
+scene and as the oracle's render of each scene, also when the launch is replayed from a CUDA
+graph."""
 import numpy as np
 import pytest
 
@@ -25,24 +26,30 @@ def _scenes(aarbf_mod):
         cam = scenes.orbit_camera(azimuth_deg=float(rng.uniform(0, 360)), elevation_deg=float(rng.uniform(-30, 30)))
         rp = scenes.native_params(cam, w, h, float(sc.radii.max()), 0.002, 300.0, dom, spp=spp, frame_id=5 * k,
                                   majorant=True, bin_length=0.008)
-        out.append((ctx, rp, (w, h)))
+        out.append((ctx, rp, (w, h), (sc, (cm, rm, dm), dom)))
     return out
 
 
-def test_batched_matches_single_renders(aarbf_mod):
+def test_batched_matches_single_renders(aarbf_mod, orc):
     import torch
     items = _scenes(aarbf_mod)
     ref = []
-    for ctx, rp, (w, h) in items:
+    for ctx, rp, (w, h), (sc, tf, dom) in items:
         acc = torch.zeros((h, w, 4), device="cuda")
         img = torch.zeros_like(acc)
         ctx.render(rp, w, h, acc, img)
         ctx.sync()
         ref.append((acc.cpu().numpy(), img.cpu().numpy()))
+        # every scene's single render equals the oracle's
+        scene = orc.build_scene(sc.xyzw, sc.radii, dom, 4, float(sc.radii.max()), tf, 1 / 255)[0]
+        oa, oi = scene.render(orc.params_from(rp), w, h)
+        assert np.array_equal(ref[-1][1].view(np.uint32), oi.view(np.uint32))
+        assert np.array_equal(ref[-1][0].view(np.uint32), oa.view(np.uint32))
     assert any((r[1][..., :3] > 0).mean() > 0.01 for r in ref)
-    accs = [torch.zeros((h, w, 4), device="cuda") for _, _, (w, h) in items]
+    accs = [torch.zeros((h, w, 4), device="cuda") for _, _, (w, h), _ in items]
     imgs = [torch.zeros_like(a) for a in accs]
-    b = aarbf_mod.Batch([c for c, _, _ in items], [p for _, p, _ in items], [s for _, _, s in items], accs, imgs)
+    b = aarbf_mod.Batch([c for c, _, _, _ in items], [p for _, p, _, _ in items], [s for _, _, s, _ in items], accs,
+                        imgs)
     for cap in (0, 512, 1024):
         for a in accs:
             a.zero_()
@@ -69,5 +76,5 @@ def test_batched_matches_single_renders(aarbf_mod):
         assert np.array_equal(i.cpu().numpy().view(np.uint32), ri.view(np.uint32))
     del g
     b.close()
-    for ctx, _, _ in items:
+    for ctx, _, _, _ in items:
         ctx.close()

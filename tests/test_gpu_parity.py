@@ -126,6 +126,35 @@ def test_domain_reduce_matches_oracle(ctx, orc):
         ctx.domain_accumulate(bad, __import__("aarbf").domain_init())
 
 
+def test_series_domain_matches_oracle(ctx, orc, aarbf_mod):
+    """the space-time box and attribute range of a whole series (hostCode.cpp:183-193, :227-240):
+    frames of different sizes that move, grow and shift their attributes, reduced frame by frame
+    on the device into one running domain; then the series' Hilbert keys of the last frame"""
+    frames = []
+    for k, n in enumerate((50_000, 20_000, 80_000)):
+        xyzw, _ = random_scene(n, 40 + k)
+        xyzw[:, :3] = xyzw[:, :3] * np.float32(1.0 + 0.5 * k) + np.float32(0.3 * k - 0.2)
+        xyzw[:, 3] = xyzw[:, 3] * np.float32(2.0) - np.float32(k)
+        frames.append(xyzw)
+    dom = aarbf_mod.domain_init()
+    for f in frames:
+        dom = ctx.domain_accumulate(f, dom)
+    want = orc.domain(frames)
+    assert_bitexact(dom, want, "series domain")
+    # no frame alone spans it
+    assert all(not np.array_equal(orc.domain([f]), want) for f in frames)
+    # the last frame quantised in the series' domain (not its own): keys and order as the oracle's
+    scene, keys, perm, _ = setup_both(ctx, orc, aarbf_mod, frames[-1], None, 1, 0.02)
+    ctx.set_domain(want)
+    ctx.build(0.02, 1)
+    scene, keys, perm = orc.build_scene(frames[-1], None, want, 1, 0.02,
+                                        orc.tf_from_rgba8(*aarbf_mod.default_transfer_functions_rgba8()))
+    gk, gp = ctx.hilbert_keys()
+    assert_bitexact(gk, keys, "hilbert keys in the series domain")
+    assert_bitexact(gp, perm, "sort permutation in the series domain")
+    assert_bitexact(ctx.sorted_particles(), scene.xyzw, "normalised attributes in the series domain")
+
+
 def reference_params(aarbf_mod, dom, w, h, **kw):
     """the reference's startup state: radius 0.01 diag, unit 0.1 radius, ambient 0.5, light 0/0,
     visualizeAttributes on, camera from the domain max looking at the centre (hostCode.cpp:252-271)"""

@@ -1,12 +1,13 @@
 """Series playback with overlapped upload/build (aarbf.streaming.SeriesRenderer): the images of
-every frame equal those of the reference's one-after-the-other order with a single context."""
+every frame equal those of the reference's one-after-the-other order with a single context, and
+both equal the oracle's render of that frame bit for bit."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
 
-def test_series_overlap_matches_sequential(aarbf_mod):
+def test_series_overlap_matches_sequential(aarbf_mod, orc):
     import torch
     from aarbf import scenes, streaming
     base = scenes.config_clusters(40_000, clusters=6, seed=31)
@@ -45,4 +46,8 @@ def test_series_overlap_matches_sequential(aarbf_mod):
         assert np.array_equal(ref.cpu().numpy().view(np.uint32), imgs[k].cpu().numpy().view(np.uint32))
         if k == 0:
             assert (ref[..., :3] > 0).float().mean() > 0.01
+        # the oracle's render of the same frame
+        scene = orc.build_scene(x, r, dom, 4, rmax, tf, 1 / 255)[0]
+        _, want = scene.render(orc.params_from(params(k)), w, h)
+        assert np.array_equal(imgs[k].cpu().numpy().view(np.uint32), want.view(np.uint32)), f"frame {k}"
     ctx.close()

@@ -62,5 +62,14 @@ def test_noalloc_sort_matches_build(aarbf_mod, orc):
         # beyond the fixed maximum: refused before any GPU work
         with pytest.raises(aarbf_mod.AarbfError):
             aarbf_mod.hilbert_sort_noalloc(0, aarbf_mod.NOALLOC_MAX_PARTICLES + 1, np.zeros(8, np.float32), 0, 0)
+        # host buffers instead of device memory: refused before any kernel is launched
+        n = 1000
+        xyzw = _scene(n, 3)
+        keys = np.zeros(n, np.uint64)
+        perm = np.zeros(n, np.uint32)
+        with pytest.raises(aarbf_mod.AarbfError):
+            aarbf_mod.hilbert_sort_noalloc(xyzw.ctypes.data, n, orc.domain([xyzw]), keys.ctypes.data,
+                                           perm.ctypes.data)
+        assert not keys.any() and not perm.any()
     finally:
         ctx.close()
