@@ -768,7 +768,14 @@ typedef struct {
   float lhs;
   int shadow;
   int marching;
+  float gap; /* smallest relative gap between the two sides of any random decision so far */
 } orc_tracker;
+
+/* records how close a decision a < b (or a > b) came to going the other way */
+static inline void note_gap(orc_tracker *tr, float a, float b) {
+  float g = fabsf(a - b) / fmaxf(fabsf(b), 1e-30f);
+  if (g < tr->gap) tr->gap = g;
+}
 
 /* sharedCode.h:151-185 */
 static int aabb_intersect(const orc_ray *r, const float *lb, const float *rt, float *tenter,
@@ -838,7 +845,9 @@ static void track_delta(const orc_scene *s, const orc_params *p, orc_tracker *tr
     sample_at(s, x, &smp);
     if (smp.count == 0) continue;
     float density = sample_density(s, p, smp.density);
-    if (orc_lcg_randomf(&tr->rng) < density / 1.0f) {
+    float xi = orc_lcg_randomf(&tr->rng);
+    note_gap(tr, xi, density / 1.0f);
+    if (xi < density / 1.0f) {
       float rgb[3];
       sample_color(s, p, &smp, rgb);
       tr->albedo[0] = rgb[0];
@@ -864,6 +873,7 @@ static void track_march(const orc_scene *s, const orc_params *p, orc_tracker *tr
     if (!(smp.count > 0 && smp.density > 0.0f)) continue;
     float density = sample_density(s, p, smp.density);
     tr->lhs = tr->lhs + density;
+    if (!tr->shadow) note_gap(tr, tr->lhs, rhs);
     if (tr->lhs > rhs && !tr->shadow) {
       float rgb[3];
       sample_color(s, p, &smp, rgb);
@@ -875,6 +885,7 @@ static void track_march(const orc_scene *s, const orc_params *p, orc_tracker *tr
     }
     if (tr->shadow) {
       tr->albedo[3] = tr->albedo[3] + (1.0f - orc_expf(-density));
+      note_gap(tr, tr->albedo[3], 1.0f);
       if (tr->albedo[3] >= 1.0f) {
         tr->albedo[3] = 1.0f;
         return;
@@ -1024,7 +1035,9 @@ static int track_bin(const orc_bin_ctx *b, float lo, float hi, int depth, float 
     orc_sample smp;
     sample_at(b->s, x, &smp);
     float sigma = smp.density * b->scale;
-    if (orc_lcg_randomf(&tr->rng) < sigma / M) {
+    float xi = orc_lcg_randomf(&tr->rng);
+    note_gap(tr, xi, sigma / M);
+    if (xi < sigma / M) {
       float rgb[3];
       sample_color(b->s, b->p, &smp, rgb);
       tr->albedo[0] = rgb[0];
@@ -1097,7 +1110,7 @@ static float noise_at(const orc_params *p, uint32_t frame, uint32_t px, uint32_t
 /* ParticleRBFRayGen, deviceCodeRBF.hlsl:206-336, one sample; returns colour (pre-accumulation)
  * and the noise value used for showNoise */
 static void raygen_sample(const orc_scene *s, const orc_params *p, const float *light, uint32_t frame,
-                          int px, int py, int w, int h, float *color, float *noise_out) {
+                          int px, int py, int w, int h, float *color, float *noise_out, float *gap_out) {
   uint32_t rng = orc_get_rng((int)frame, (uint32_t)px, (uint32_t)py, (uint32_t)w);
   float sx = ((float)px + 0.5f + p->jitter_x) / (float)w;
   float sy = ((float)py + 0.5f + p->jitter_y) / (float)h;
@@ -1136,6 +1149,7 @@ static void raygen_sample(const orc_scene *s, const orc_params *p, const float *
   tr.lhs = 0.0f;
   tr.random = rnd[0];
   tr.shadow = 0;
+  tr.gap = INFINITY;
   float col[4] = {0, 0, 0, 0};
   *noise_out = rnd[0];
 
@@ -1172,20 +1186,23 @@ static void raygen_sample(const orc_scene *s, const orc_params *p, const float *
   }
   float bg[4] = {0.0f, 0.0f, 0.0f, 1.0f};
   over(col, bg, color);
+  *gap_out = tr.gap;
 }
 
 static void render_pixel(const orc_scene *s, const orc_params *p, const float *light, int px,
-                         int py, int w, int h, float *accum, float *image) {
+                         int py, int w, int h, float *accum, float *image, float *gaps) {
   size_t ofs = (size_t)py * (size_t)w + (size_t)px;
   float prev[4] = {accum[4 * ofs], accum[4 * ofs + 1], accum[4 * ofs + 2], accum[4 * ofs + 3]};
   float fin[4] = {prev[0], prev[1], prev[2], prev[3]};
   float noise = 0.0f;
   uint32_t spp = p->spp ? p->spp : 1;
+  float gap = INFINITY;
   for (uint32_t k = 0; k < spp; ++k) {
     uint32_t frame = (p->frame_id + k) & 0xffffu;
     uint32_t aid = (p->accum_id + k) & 0xffffu;
-    float color[4];
-    raygen_sample(s, p, light, frame, px, py, w, h, color, &noise);
+    float color[4], g;
+    raygen_sample(s, p, light, frame, px, py, w, h, color, &noise, &g);
+    if (g < gap) gap = g;
     /* deviceCodeRBF.hlsl:326-328 */
     float fa = (float)aid;
     float wa = 1.0f / fa, wb = (float)((int)aid - 1) / fa;
@@ -1198,10 +1215,11 @@ static void render_pixel(const orc_scene *s, const orc_params *p, const float *l
     fin[3] = 1.0f;
   }
   memcpy(image + 4 * ofs, fin, sizeof(fin));
+  if (gaps) gaps[ofs] = gap;
 }
 
-void orc_render_region(const orc_scene *s, const orc_params *p, int w, int h, int x0, int x1,
-                       int y0, int y1, float *accum, float *image, int nthreads) {
+void orc_render_region_gaps(const orc_scene *s, const orc_params *p, int w, int h, int x0, int x1,
+                            int y0, int y1, float *accum, float *image, float *gaps, int nthreads) {
   float light[3];
   orc_light_dir(p->light_azimuth, p->light_elevation, light);
   int nt = nthreads > 0 ? nthreads : g_threads;
@@ -1212,9 +1230,14 @@ void orc_render_region(const orc_scene *s, const orc_params *p, int w, int h, in
 #endif
   for (long k = 0; k < total; ++k) {
     int py = y0 + (int)(k / cols), px = x0 + (int)(k % cols);
-    render_pixel(s, p, light, px, py, w, h, accum, image);
+    render_pixel(s, p, light, px, py, w, h, accum, image, gaps);
   }
   (void)nt;
+}
+
+void orc_render_region(const orc_scene *s, const orc_params *p, int w, int h, int x0, int x1,
+                       int y0, int y1, float *accum, float *image, int nthreads) {
+  orc_render_region_gaps(s, p, w, h, x0, x1, y0, y1, accum, image, NULL, nthreads);
 }
 
 void orc_render(const orc_scene *s, const orc_params *p, int w, int h, float *accum, float *image,

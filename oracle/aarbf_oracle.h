@@ -131,6 +131,12 @@ void orc_render(const orc_scene *s, const orc_params *p, int w, int h, float *ac
 /* render only rows [y0,y1) x cols [x0,x1) (bounded CPU-baseline samples) */
 void orc_render_region(const orc_scene *s, const orc_params *p, int w, int h, int x0, int x1,
                        int y0, int y1, float *accum, float *image, int nthreads);
+/* the same, plus per pixel (w x h, written inside the region) the smallest relative gap
+ * |a - b| / |b| between the two sides of any random decision its samples took (the collision
+ * test, the marching threshold, the shadow opacity cap): a pixel whose gap is tiny can change
+ * with the rounding of the reference's float any-hit sums, whose order the hardware decides */
+void orc_render_region_gaps(const orc_scene *s, const orc_params *p, int w, int h, int x0, int x1,
+                            int y0, int y1, float *accum, float *image, float *gaps, int nthreads);
 void orc_render_splat(const orc_scene *s, const orc_params *p, int w, int h, float *image,
                       int nthreads);
 /* CompositeGui TAA (deviceCodeCommon.hlsl:67-115); bgra may be NULL */

@@ -87,6 +87,8 @@ def lib():
             "orc_point_query_brute": ([P, P, P], i32),
             "orc_render": ([P, ctypes.POINTER(OrcParams), i32, i32, P, P, i32], None),
             "orc_render_region": ([P, ctypes.POINTER(OrcParams), i32, i32, i32, i32, i32, i32, P, P, i32], None),
+            "orc_render_region_gaps": ([P, ctypes.POINTER(OrcParams), i32, i32, i32, i32, i32, i32, P, P, P, i32],
+                                       None),
             "orc_render_splat": ([P, ctypes.POINTER(OrcParams), i32, i32, P, i32], None),
             "orc_taa": ([P, P, P, P, i32, i32, i32], None),
             "orc_set_threads": ([i32], None),
@@ -228,6 +230,16 @@ class Scene:
             lib().orc_render_region(self.h, ctypes.byref(params), w, h, x0, x1, y0, y1, _p(accum),
                                     _p(image), threads)
         return accum, image
+
+    def render_gaps(self, params, w, h, accum=None, threads=0):
+        """render() of the whole frame plus, per pixel, the smallest relative gap between the two
+        sides of any random decision its samples took (see orc_render_region_gaps)."""
+        accum = np.zeros((h, w, 4), np.float32) if accum is None else np.ascontiguousarray(accum, np.float32)
+        image = np.zeros((h, w, 4), np.float32)
+        gaps = np.full((h, w), np.inf, np.float32)
+        lib().orc_render_region_gaps(self.h, ctypes.byref(params), w, h, 0, w, 0, h, _p(accum), _p(image), _p(gaps),
+                                     threads)
+        return accum, image, gaps
 
     def render_f64(self, params, w, h, region, spp, clamp_plain=False, seed=1, threads=0):
         """FP64 twin of the native volume model: mean RGB over spp samples of the region

@@ -1,9 +1,13 @@
 """Generate the golden vectors in tests/golden/ from the reference's own code.
 
-Runs in a container that has the reference tree: oracle/Makefile compiles the reference's
-hilbert.h and rng.h unchanged into oracle/_ref/libaarbf_ref.so; this script calls it and writes
-hilbert_rng.json. The CPU tests pin the oracle's restatements against these vectors (on machines
-without the reference tree) and against the live reference library (where it exists).
+Runs in a container that has the reference tree ($AARBF_REFERENCE, else the read-only tree this
+build environment mounts): oracle/Makefile compiles the reference's hilbert.h and rng.h unchanged
+into oracle/_ref/libaarbf_ref.so, and its HLSL device programs (rewritten to C++ by
+oracle/hlsl/hlsl2cpp.py, run on the GPRT stand-in oracle/hlsl/gprt.h) into
+oracle/_ref/libaarbf_hlsl_ref.so. This script calls them and writes hilbert_rng.json and
+hlsl_ref.npz (the reference programs' outputs on the cases of hlsl_cases.py). The CPU tests pin
+the oracle's restatements against these fixtures (on machines without the reference tree) and
+against the live reference libraries (where they exist).
 
     python tests/golden/make_golden.py
 """
@@ -18,8 +22,55 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 REF = os.path.join(ROOT, "oracle", "_ref", "libaarbf_ref.so")
 
 
+def reference_tree():
+    for cand in (os.environ.get("AARBF_REFERENCE"), "/root/reference"):
+        if cand and os.path.isfile(os.path.join(cand, "hilbert.h")):
+            return cand
+    raise SystemExit("reference tree not found (set AARBF_REFERENCE)")
+
+
+def write_hlsl_golden():
+    """the reference's device programs on every case of hlsl_cases.py -> hlsl_ref.npz"""
+    import sys
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "attribute-aware-rbfs_b200"))
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import hlsl_cases as hc
+    import oracle.href as href
+    import oracle.oracle as orc
+    out = {}
+    for name, case in hc.cases().items():
+        if case["kind"] == "taa":
+            img, prev = hc.taa_inputs(case["seed"])
+            for d in (0, 1):
+                taa, bgra = href.taa(img, prev, disable=bool(d))
+                if not d:
+                    out[f"{name}_taa"] = taa
+                out[f"{name}_bgra{d}"] = bgra
+            continue
+        sc, tf, p, r, accum0, atlas = hc.inputs(orc, case)
+        boxes = href.bounds(sc.xyzw, case["ppl"], r, tf[1])
+        if case["kind"] == "bounds":
+            out[name] = boxes
+        elif case["kind"] == "render":
+            acc, img = href.render(sc.xyzw, boxes, case["ppl"], p, tf, hc.W, hc.H, accum=accum0, stbn=atlas)
+            out[f"{name}_accum"], out[f"{name}_image"] = acc, img
+            # the same launches with the leaves visited in reverse order: pixels that differ
+            # depend on the hardware's (unspecified) any-hit order
+            _, img_rev = href.render(sc.xyzw, boxes, case["ppl"], p, tf, hc.W, hc.H, accum=accum0, stbn=atlas,
+                                     reverse=True)
+            out[f"{name}_image_reverse"] = img_rev
+        else:
+            out[f"{name}_image"] = href.render_splat(sc.xyzw, boxes, case["ppl"], p, tf, hc.W, hc.H)
+    path = os.path.join(ROOT, "tests", "golden", "hlsl_ref.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, len(out), "arrays")
+
+
 def main():
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    ref = reference_tree()
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"REF={ref}"], check=True)
+    write_hlsl_golden()
     L = ctypes.CDLL(REF)
     ull = ctypes.c_ulonglong
     L.ref_hilbert_c2i.restype = ull
