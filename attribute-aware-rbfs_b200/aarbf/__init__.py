@@ -32,9 +32,9 @@ FLAG_DENSITY_LINEAR = 1 << 4
 FLAG_SPLAT_PARTICLE_RADIUS = 1 << 5
 FLAG_MAJORANT_TRACKING = 1 << 6
 
-TRAVERSAL_AUTO = 0      # majorant tracking: one warp per ray; otherwise per-thread staged
-TRAVERSAL_STAGED = 0
-TRAVERSAL_POINT = 1     # one BVH point query per tracking step
+TRAVERSAL_AUTO = 0      # one warp per ray (warp-wide traversal, staged candidate lists) for every estimator
+TRAVERSAL_STAGED = 0    # the same (staged candidates; kept name)
+TRAVERSAL_POINT = 1     # one BVH point query per tracking step, one thread per sample
 TRAVERSAL_THREAD = 2    # per-thread staged segments for every estimator
 
 STORAGE_FP32 = 0
@@ -42,9 +42,10 @@ STORAGE_FP16 = 1        # FP16 positions (relative to 256-particle run origins),
 
 
 def uses_warp_kernel(p) -> bool:
-    """True when a render with these parameters runs a ray-per-warp kernel: majorant tracking or
-    stochastic marching (blue-noise mode) with the default traversal."""
-    return int(p.traversal) == TRAVERSAL_AUTO and bool(p.flags & (FLAG_MAJORANT_TRACKING | FLAG_BLUE_NOISE))
+    """True when a render with these parameters runs a ray-per-warp kernel: every estimator (the
+    reference's delta tracking, delta tracking with per-bin majorants, stochastic marching) with
+    the default traversal."""
+    return int(p.traversal) == TRAVERSAL_AUTO
 
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "out of memory", 3: "CUDA error",
@@ -57,7 +58,7 @@ EXPORTED_SYMBOLS = (
     "aarbf_sync", "aarbf_set_particles", "aarbf_set_domain", "aarbf_domain_init",
     "aarbf_domain_accumulate", "aarbf_set_transfer_functions_rgba8",
     "aarbf_set_transfer_functions_f32", "aarbf_marks_to_rgba8", "aarbf_build", "aarbf_refit",
-    "aarbf_render", "aarbf_render_splat", "aarbf_taa_resolve", "aarbf_get_framebuffers",
+    "aarbf_refit_frame", "aarbf_render", "aarbf_render_splat", "aarbf_taa_resolve", "aarbf_get_framebuffers",
     "aarbf_set_noise_atlas", "aarbf_generate_noise_atlas", "aarbf_camera", "aarbf_series_load",
     "aarbf_series_num_frames", "aarbf_series_frame", "aarbf_series_free", "aarbf_series_save",
     "aarbf_get_num_particles", "aarbf_get_hilbert_keys", "aarbf_get_sorted_particles",
@@ -112,6 +113,7 @@ def _load():
         "aarbf_marks_to_rgba8": [P, P, i32, i32, P, i32],
         "aarbf_build": [P, f32, u32, P],
         "aarbf_refit": [P, f32, P],
+        "aarbf_refit_frame": [P, i32, P],
         "aarbf_render": [P, ctypes.POINTER(Params), i32, i32, P, P, P],
         "aarbf_render_splat": [P, ctypes.POINTER(Params), i32, i32, P, P],
         "aarbf_taa_resolve": [P, P, P, P, P, i32, i32, i32, P],
@@ -387,6 +389,11 @@ class Context:
 
     def refit(self, rbf_radius: float, stream=None):
         self._check(self._lib.aarbf_refit(self._h, float(rbf_radius), _stream_ptr(stream)))
+
+    def refit_frame(self, keep_order: bool = False, stream=None):
+        """aarbf_refit_frame: the frame set by set_particles refits the last build's BVH topology
+        (the reference's update on a frame change)."""
+        self._check(self._lib.aarbf_refit_frame(self._h, int(bool(keep_order)), _stream_ptr(stream)))
 
     # -- launches ------------------------------------------------------------------------
     def render(self, params: RenderParams, width: int, height: int, accum=None, image=None,

@@ -247,6 +247,8 @@ struct aarbf_ctx {
   uint32_t ppl = 1, nleaves = 0;
   float rbf_radius = 0.0f;
   bool built = false;
+  uint64_t built_n = 0;          // particle count and radii presence of the last aarbf_build
+  bool built_has_radii = false;
   float root_box_host[6] = {0, 0, 0, 0, 0, 0};
   // transfer functions
   aarbf::DevBuf tf_color, tf_radius, tf_density;

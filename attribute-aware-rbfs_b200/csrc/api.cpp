@@ -294,6 +294,76 @@ aarbf_status ensure_fb(aarbf_ctx* ctx, int w, int h) {
   return AARBF_OK;
 }
 
+// the frame's Hilbert keys and sort permutation (ctx->sorted_keys, ctx->perm), as the reference
+// sorts each frame along the curve of the space-time box (hostCode.cpp:195-222)
+aarbf_status sort_frame(aarbf_ctx* ctx, const float* dom, cudaStream_t st) {
+  const uint64_t n = ctx->n;
+  const float4* in = ctx->in_xyzw.as<float4>();
+  uint64_t* keys = ctx->keys.as<uint64_t>();
+  uint32_t* perm = ctx->perm.as<uint32_t>();
+  const size_t hw = ctx->hist.bytes / 4;
+  bool alt = false;
+  {
+    CK(launch_hilbert_keys(in, n, dom, keys, perm, st), "hilbert keys");
+    CK(radix_sort_pairs(keys, perm, ctx->keys_alt.as<uint64_t>(), ctx->perm_alt.as<uint32_t>(), n, 48,
+                        ctx->hist.as<uint32_t>(), hw, st, &alt),
+       "radix sort");
+    if (alt) {
+      keys = ctx->keys_alt.as<uint64_t>();
+      perm = ctx->perm_alt.as<uint32_t>();
+    }
+    // equal keys: short runs are ordered in place; a run longer than the in-place limit redoes
+    // the sort as an LSD chain over (w, z, y, x) then the key, each pass stable
+    CK(cudaMemsetAsync(ctx->flag.ptr, 0, 4, st), "flag");
+    CK(launch_tie_runs(keys, in, perm, n, ctx->flag.as<uint32_t>(), st), "tie runs");
+    uint32_t tie = 0;
+    CK(cudaMemcpyAsync(&tie, ctx->flag.ptr, 4, cudaMemcpyDeviceToHost, st), "tie read");
+    CK(cudaStreamSynchronize(st), "tie sync");
+    if (tie & 2u) {
+      uint64_t* k0 = ctx->keys.as<uint64_t>();
+      uint64_t* k1 = ctx->keys_alt.as<uint64_t>();
+      uint32_t* p0 = ctx->perm.as<uint32_t>();
+      uint32_t* p1 = ctx->perm_alt.as<uint32_t>();
+      // identity permutation via a key pass with ident output
+      CK(launch_hilbert_keys(in, n, dom, k0, p0, st), "ident");
+      for (int comp = 3; comp >= -1; --comp) {
+        if (comp >= 0) CK(launch_orderable_component(in, p0, n, comp, k0, st), "tie keys");
+        else CK(launch_hilbert_keys_perm(in, p0, n, dom, k0, st), "tie keys");
+        bool a2 = false;
+        CK(radix_sort_pairs(k0, p0, k1, p1, n, comp >= 0 ? 32 : 48, ctx->hist.as<uint32_t>(), hw, st, &a2),
+           "tie sort");
+        if (a2) {
+          uint64_t* tk = k0; k0 = k1; k1 = tk;
+          uint32_t* tp = p0; p0 = p1; p1 = tp;
+        }
+      }
+      keys = k0;
+      perm = p0;
+    }
+    CK(cudaMemcpyAsync(ctx->sorted_keys.ptr, keys, 8 * n, cudaMemcpyDeviceToDevice, st), "keys");
+    if (perm != ctx->perm.as<uint32_t>())
+      CK(cudaMemcpyAsync(ctx->perm.ptr, perm, 4 * n, cudaMemcpyDeviceToDevice, st), "perm");
+  }
+  return AARBF_OK;
+}
+
+// the frame's particles in the order of ctx->perm, attributes normalised over dom; FP16 records
+aarbf_status gather_frame(aarbf_ctx* ctx, const float* dom, cudaStream_t st) {
+  const uint64_t n = ctx->n, nn = n ? n : 1;
+  CK(launch_gather_normalize(ctx->in_xyzw.as<float4>(), ctx->has_radii ? ctx->in_radii.as<float>() : nullptr,
+                             ctx->perm.as<uint32_t>(), n, dom[6], dom[7], ctx->xyzw.as<float4>(),
+                             ctx->radii.as<float>(), st),
+     "gather");
+  if (ctx->storage_fp16) {
+    CK(ctx->posq.reserve(8 * nn), "alloc");
+    CK(ctx->colq.reserve(8 * nn), "alloc");
+    CK(ctx->reval.reserve(4 * nn), "alloc");
+    CK(ctx->origin.reserve(16 * ((nn + 255) / 256)), "alloc");
+    CK(launch_quantize_positions(ctx->xyzw.as<float4>(), n, ctx->posq.as<uint2>(), ctx->origin.as<float4>(), st),
+       "fp16 positions");
+  }
+  return AARBF_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -544,73 +614,47 @@ aarbf_status aarbf_build(aarbf_ctx* ctx, float rbf_radius, uint32_t ppl, void* s
   CK(ctx->root_box.reserve(64), "alloc");
   CK(ctx->sorted_keys.reserve(8 * nn), "alloc");
 
-  const float4* in = ctx->in_xyzw.as<float4>();
-  uint64_t* keys = ctx->keys.as<uint64_t>();
-  uint32_t* perm = ctx->perm.as<uint32_t>();
-  const size_t hw = ctx->hist.bytes / 4;
-  bool alt = false;
   if (n) {
-    CK(launch_hilbert_keys(in, n, dom, keys, perm, st), "hilbert keys");
-    CK(radix_sort_pairs(keys, perm, ctx->keys_alt.as<uint64_t>(), ctx->perm_alt.as<uint32_t>(), n, 48,
-                        ctx->hist.as<uint32_t>(), hw, st, &alt),
-       "radix sort");
-    if (alt) {
-      keys = ctx->keys_alt.as<uint64_t>();
-      perm = ctx->perm_alt.as<uint32_t>();
-    }
-    // equal keys: short runs are ordered in place; a run longer than the in-place limit redoes
-    // the sort as an LSD chain over (w, z, y, x) then the key, each pass stable
-    CK(cudaMemsetAsync(ctx->flag.ptr, 0, 4, st), "flag");
-    CK(launch_tie_runs(keys, in, perm, n, ctx->flag.as<uint32_t>(), st), "tie runs");
-    uint32_t tie = 0;
-    CK(cudaMemcpyAsync(&tie, ctx->flag.ptr, 4, cudaMemcpyDeviceToHost, st), "tie read");
-    CK(cudaStreamSynchronize(st), "tie sync");
-    if (tie & 2u) {
-      uint64_t* k0 = ctx->keys.as<uint64_t>();
-      uint64_t* k1 = ctx->keys_alt.as<uint64_t>();
-      uint32_t* p0 = ctx->perm.as<uint32_t>();
-      uint32_t* p1 = ctx->perm_alt.as<uint32_t>();
-      // identity permutation via a key pass with ident output
-      CK(launch_hilbert_keys(in, n, dom, k0, p0, st), "ident");
-      for (int comp = 3; comp >= -1; --comp) {
-        if (comp >= 0) CK(launch_orderable_component(in, p0, n, comp, k0, st), "tie keys");
-        else CK(launch_hilbert_keys_perm(in, p0, n, dom, k0, st), "tie keys");
-        bool a2 = false;
-        CK(radix_sort_pairs(k0, p0, k1, p1, n, comp >= 0 ? 32 : 48, ctx->hist.as<uint32_t>(), hw, st, &a2),
-           "tie sort");
-        if (a2) {
-          uint64_t* tk = k0; k0 = k1; k1 = tk;
-          uint32_t* tp = p0; p0 = p1; p1 = tp;
-        }
-      }
-      keys = k0;
-      perm = p0;
-    }
-    CK(cudaMemcpyAsync(ctx->sorted_keys.ptr, keys, 8 * n, cudaMemcpyDeviceToDevice, st), "keys");
-    if (perm != ctx->perm.as<uint32_t>())
-      CK(cudaMemcpyAsync(ctx->perm.ptr, perm, 4 * n, cudaMemcpyDeviceToDevice, st), "perm");
-    CK(launch_gather_normalize(in, ctx->has_radii ? ctx->in_radii.as<float>() : nullptr, ctx->perm.as<uint32_t>(), n,
-                               dom[6], dom[7], ctx->xyzw.as<float4>(), ctx->radii.as<float>(), st),
-       "gather");
-    if (ctx->storage_fp16) {
-      CK(ctx->posq.reserve(8 * nn), "alloc");
-      CK(ctx->colq.reserve(8 * nn), "alloc");
-      CK(ctx->reval.reserve(4 * nn), "alloc");
-      CK(ctx->origin.reserve(16 * ((nn + 255) / 256)), "alloc");
-      CK(launch_quantize_positions(ctx->xyzw.as<float4>(), n, ctx->posq.as<uint2>(), ctx->origin.as<float4>(), st),
-         "fp16 positions");
-    }
+    aarbf_status s = sort_frame(ctx, dom, st);
+    if (s != AARBF_OK) return s;
+    s = gather_frame(ctx, dom, st);
+    if (s != AARBF_OK) return s;
     CK(launch_karras(ctx->sorted_keys.as<uint64_t>(), n, ppl, ctx->nleaves, ctx->nodes.as<Node>(),
                      ctx->nodes_ref.as<Node>(), ctx->leaf_parent.as<uint32_t>(), st),
        "karras");
   }
   memcpy(ctx->dom, dom, sizeof(dom));
   ctx->built_fp16 = ctx->storage_fp16 && n > 0;
+  ctx->built_n = n;
+  ctx->built_has_radii = ctx->has_radii;
   aarbf_status s = run_refit(ctx, st);
   if (s != AARBF_OK) return s;
   if (!n)
     for (int a = 0; a < 6; ++a) ctx->root_box_host[a] = NAN;
   return AARBF_OK;
+}
+
+
+aarbf_status aarbf_refit_frame(aarbf_ctx* ctx, int keep_order, void* stream) {
+  if (!ctx) return AARBF_ERR_INVALID_ARGUMENT;
+  if (!ctx->built || !ctx->nodes.ptr) return fail(ctx, AARBF_ERR_NOT_READY, "refit_frame before build");
+  if (ctx->n != ctx->built_n || ctx->has_radii != ctx->built_has_radii)
+    return fail(ctx, AARBF_ERR_INVALID_ARGUMENT,
+                "refit_frame needs a frame of the built particle count (and radii iff the build had them); "
+                "call aarbf_build for a new count");
+  if (ctx->storage_fp16 != ctx->built_fp16 && ctx->n)
+    return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "storage form changed since the build: call aarbf_build");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (ctx->n) {
+    if (!keep_order) {
+      aarbf_status s = sort_frame(ctx, ctx->dom, st);
+      if (s != AARBF_OK) return s;
+    }
+    aarbf_status s = gather_frame(ctx, ctx->dom, st);
+    if (s != AARBF_OK) return s;
+  }
+  return run_refit(ctx, st);
 }
 
 aarbf_status aarbf_refit(aarbf_ctx* ctx, float rbf_radius, void* stream) {

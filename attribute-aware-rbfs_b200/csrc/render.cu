@@ -1011,6 +1011,7 @@ struct WarpStager {
     int first, last;
     range(kbin, first, last);
     sample_clear(acc);
+    if (first >= last) return;  // no candidate in this bin (warp-uniform): nothing to sum
     for (int p = first + (int)(threadIdx.x & 31u); p < last; p += 32) {
       int j = slot(p);
       if (t < buf->lo[j] || t > buf->hi[j]) continue;
@@ -1213,6 +1214,80 @@ Tracker track_majorant_warp(const RenderLaunch& L, Tracker tr, const Ray ray, ui
   return tr;
 }
 
+// stochasticTracking (deviceCodeRBF.hlsl:141-203) with the warp: the reference's step sequence
+// (t -= log(1 - xi) unit with the global majorant 1, then the collision draw only where a particle
+// holds the step point) runs uniformly on every lane with the reference's draw order; the density
+// at a step point is a lane-parallel fixed-point sum over the particles staged for the point's bin
+// (bins of bin_length along the ray, staged by warp traversals as in the majorant tracker), so
+// every float equals the sequential tracker's. A bin with more candidates than the buffer takes
+// direct warp point queries. Out of line for the same reason as the majorant tracker.
+template <int CAPW, bool COUNT>
+__device__ __forceinline__ void track_delta_warp_body(const RenderLaunch& L, Tracker& tr, const Ray& ray,
+                                                      bool from_entry, WarpBuf<CAPW>* buf, uint32_t* stk) {
+  WarpStager<CAPW> st;
+  st.buf = buf;
+  st.stk = stk;
+  unsigned long long* const ctr = COUNT ? L.counters : nullptr;
+  st.ctr = ctr;
+  st.init(L.s, ray);
+  if (!from_entry) tr.t = ray.tmin;
+  const float t0 = tr.t;
+  const float Lb = L.bin_length > 0.0f ? L.bin_length : 16.0f * L.unit;  // staging granularity only
+  int seg_begin = 0, seg_end = 0;  // staged bins [seg_begin, seg_end)
+  int nb = L.stage_bins;
+  bool direct = false;
+  for (; tr.i < kMaxDepth; ++tr.i) {
+    wctr(ctr, kWcSteps, 1);
+    const float u = lcg_f(tr.rng);
+    const float step = (dlog(1.0f - u) / 1.0f) * L.unit;
+    tr.t = tr.t - step;
+    if (tr.t >= ray.tmax) return;
+    const float t = tr.t;
+    // outside the (inflated) root box no particle holds the step point
+    if (t < st.rb_enter || t > st.rb_exit) continue;
+    const float fk = floorf((t - t0) / Lb);
+    const int kb = fk < 1.0e9f ? (int)fk : 1000000000;
+    if (kb < seg_begin || kb >= seg_end) {
+      direct = false;
+      for (;;) {
+        if (st.stage(L.s, ray, kb, nb, t0, Lb, L.status)) {
+          seg_begin = kb;
+          seg_end = kb + nb;
+          if (nb < kMaxSegBins) nb *= 2;
+          break;
+        }
+        nb >>= 1;
+        if (nb == 0) {
+          direct = true;
+          seg_begin = kb;
+          seg_end = kb + 1;
+          nb = 1;
+          break;
+        }
+      }
+    }
+    const float3 x = make_float3(ray.o.x + t * ray.d.x, ray.o.y + t * ray.d.y, ray.o.z + t * ray.d.z);
+    Sample smp;
+    if (direct) smp = warp_point<CAPW>(L.s, x, buf, stk, L.status, ctr);
+    else st.sample(L.s, kb, t, x, smp);
+    if (smp.count == 0) continue;
+    const float D = (float)smp.a0 * kFixInv;
+    const float density = sample_density(L, D);
+    if (lcg_f(tr.rng) < density / 1.0f) {
+      const float3 c = sample_color(L, smp, D);
+      tr.albedo = make_float4(c.x, c.y, c.z, 1.0f);
+      return;
+    }
+  }
+}
+
+template <int CAPW, bool COUNT>
+__device__ __noinline__ Tracker track_delta_warp(const RenderLaunch& L, Tracker tr, const Ray ray, bool from_entry,
+                                                 uint32_t* stk) {
+  track_delta_warp_body<CAPW, COUNT>(L, tr, ray, from_entry, warp_buf<CAPW>(), stk);
+  return tr;
+}
+
 // stochasticMarching (deviceCodeRBF.hlsl:67-139) with the warp: the steps of a chunk (up to 32)
 // are evaluated one per lane against the particles staged for the chunk's segment; the step
 // positions are the reference's running sum t += unit and the accumulated density / shadow
@@ -1386,11 +1461,14 @@ __device__ __forceinline__ uint32_t warp_items(const RenderLaunch& L) {
   return tiles_x * ((uint32_t)(L.height + 3) / 4u) * 32u * spp;
 }
 
-// one work item of the ray-per-warp kernel (all lanes of the warp); MARCH: stochastic marching
-// (blue-noise mode), else delta tracking with per-bin majorants, each in its own kernel so neither
-// carries the other's code; COUNT: the count-mode instance (render_count), so the timed instance
-// carries no accounting code
-template <int CAPW, bool MARCH, bool COUNT>
+// estimators of the ray-per-warp kernel, each in its own kernel instance so none carries another's
+// code: delta tracking with per-bin majorants (native), stochastic marching (blue-noise mode), and
+// the reference's delta tracking with the global majorant
+enum { kWarpMajorant = 0, kWarpMarch = 1, kWarpDelta = 2 };
+
+// one work item of the ray-per-warp kernel (all lanes of the warp); COUNT: the count-mode instance
+// (render_count), so the timed instance carries no accounting code
+template <int CAPW, int MODE, bool COUNT>
 __device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t item, WarpBuf<CAPW>* buf,
                                                  uint32_t* stk) {
   const uint32_t lane = threadIdx.x & 31u;
@@ -1406,11 +1484,12 @@ __device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t
   const size_t ofs = (size_t)px + (size_t)L.width * (size_t)py;
   const long long c0 = cost ? clock64() : 0;
   float noise = 0.0f;
-  float4 c = raygen_generic<MARCH ? 1 : 0>(L, (L.frame_id + k) & 0xffffu, px, py, noise, COUNT && lane == 0,
-                            [&](Tracker& tr, const Ray& r, bool) {
-                              if (MARCH) tr = track_march_warp<CAPW>(L, tr, r, stk);
-                              else tr = track_majorant_warp<CAPW, COUNT>(L, tr, r, stk);
-                            });
+  float4 c = raygen_generic<MODE == kWarpMarch ? 1 : 0>(
+      L, (L.frame_id + k) & 0xffffu, px, py, noise, COUNT && lane == 0, [&](Tracker& tr, const Ray& r, bool from_entry) {
+        if (MODE == kWarpMarch) tr = track_march_warp<CAPW>(L, tr, r, stk);
+        else if (MODE == kWarpDelta) tr = track_delta_warp<CAPW, COUNT>(L, tr, r, from_entry, stk);
+        else tr = track_majorant_warp<CAPW, COUNT>(L, tr, r, stk);
+      });
   if (cost) c.w = (float)(clock64() - c0);
   if (lane == 0) {
     L.samples[(size_t)k * plane + ofs] = c;
@@ -1418,7 +1497,7 @@ __device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t
   }
 }
 
-template <int CAPW, bool MARCH, bool COUNT>
+template <int CAPW, int MODE, bool COUNT>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks) k_render_warp(const __grid_constant__ RenderLaunch L) {
   extern __shared__ __align__(16) char smem[];
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
@@ -1430,7 +1509,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks) k_render_
     if (lane == 0) item = atomicAdd(L.work_counter, 1u);
     item = __shfl_sync(kFull, item, 0);
     if (item >= total) break;
-    render_warp_item<CAPW, MARCH, COUNT>(L, item, buf, stk);
+    render_warp_item<CAPW, MODE, COUNT>(L, item, buf, stk);
   }
 }
 
@@ -1456,7 +1535,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks)
       if (item_ofs[mid] <= item) lo = mid;
       else hi = mid;
     }
-    render_warp_item<CAPW, false, false>(Ls[lo], (uint32_t)(item - item_ofs[lo]), buf, stk);
+    render_warp_item<CAPW, kWarpMajorant, false>(Ls[lo], (uint32_t)(item - item_ofs[lo]), buf, stk);
   }
 }
 
@@ -1590,20 +1669,20 @@ cudaError_t warp_grid(int* blocks) {
   return per_device(cache, blocks, [](int dev, int* v) {
     const int smem = (int)(sizeof(WarpBuf<CAPW>) * kWarpsPerBlock);
     const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    cudaError_t e = cudaFuncSetAttribute(k_render_warp<CAPW, false, false>, attr, smem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_render_warp<CAPW, false, true>, attr, smem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_render_warp<CAPW, true, false>, attr, smem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_render_warp<CAPW, true, true>, attr, smem);
+    cudaError_t e = cudaSuccess;
+    for (auto f : {k_render_warp<CAPW, kWarpMajorant, false>, k_render_warp<CAPW, kWarpMajorant, true>,
+                   k_render_warp<CAPW, kWarpMarch, false>, k_render_warp<CAPW, kWarpMarch, true>,
+                   k_render_warp<CAPW, kWarpDelta, false>, k_render_warp<CAPW, kWarpDelta, true>})
+      if (e == cudaSuccess) e = cudaFuncSetAttribute(f, attr, smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_render_warp_batched<CAPW>, attr, smem);
-    int sms = 0, per_sm = 0, per_m = 0;
+    int sms = 0, per_sm = 0;
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_warp<CAPW, false, false>,
-                                                        kWarpsPerBlock * 32, smem);
-    if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_m, k_render_warp<CAPW, true, false>,
-                                                        kWarpsPerBlock * 32, smem);
-    per_sm = per_m > per_sm ? per_m : per_sm;
+    for (auto f : {k_render_warp<CAPW, kWarpMajorant, false>, k_render_warp<CAPW, kWarpMarch, false>,
+                   k_render_warp<CAPW, kWarpDelta, false>}) {
+      int per = 0;
+      if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, f, kWarpsPerBlock * 32, smem);
+      per_sm = per > per_sm ? per : per_sm;
+    }
     *v = sms * (per_sm > 0 ? per_sm : 1);
     return e;
   });
@@ -1617,14 +1696,16 @@ cudaError_t launch_warp(const RenderLaunch& L, cudaStream_t st, const cudaEvent_
   e = cudaMemsetAsync(L.work_counter, 0, sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
   if (marks) cudaEventRecord(marks[0], st);
-  if ((L.flags & kFlagBlueNoise) && L.counters)
-    k_render_warp<CAPW, true, true><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
-  else if (L.flags & kFlagBlueNoise)
-    k_render_warp<CAPW, true, false><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
-  else if (L.counters)
-    k_render_warp<CAPW, false, true><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
-  else
-    k_render_warp<CAPW, false, false><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(L);
+  const size_t smem = sizeof(WarpBuf<CAPW>) * kWarpsPerBlock;
+  const int mode = (L.flags & kFlagBlueNoise) ? kWarpMarch : (L.flags & kFlagMajorantTracking) ? kWarpMajorant
+                                                                                                  : kWarpDelta;
+  auto f = L.counters ? (mode == kWarpMarch ? k_render_warp<CAPW, kWarpMarch, true>
+                         : mode == kWarpDelta ? k_render_warp<CAPW, kWarpDelta, true>
+                                              : k_render_warp<CAPW, kWarpMajorant, true>)
+                      : (mode == kWarpMarch ? k_render_warp<CAPW, kWarpMarch, false>
+                         : mode == kWarpDelta ? k_render_warp<CAPW, kWarpDelta, false>
+                                              : k_render_warp<CAPW, kWarpMajorant, false>);
+  f<<<blocks, kWarpsPerBlock * 32, smem, st>>>(L);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (marks) cudaEventRecord(marks[1], st);
@@ -1636,9 +1717,7 @@ cudaError_t launch_warp(const RenderLaunch& L, cudaStream_t st, const cudaEvent_
 
 }  // namespace
 
-bool render_uses_warp_kernel(const RenderLaunch& L) {
-  return L.traversal == AARBF_TRAVERSAL_AUTO && ((L.flags & kFlagMajorantTracking) || (L.flags & kFlagBlueNoise));
-}
+bool render_uses_warp_kernel(const RenderLaunch& L) { return L.traversal == AARBF_TRAVERSAL_AUTO; }
 
 cudaError_t render_warp_stack_words(size_t* words) {
   // enough stacks for the largest grid of any buffer depth

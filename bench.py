@@ -285,9 +285,7 @@ def traversal_label(args):
         return "point queries per step (thread per sample)"
     if args.traversal == 2:
         return "staged segments (thread per sample)"
-    if args.estimator == "majorant":
-        return "ray per warp (warp-wide BVH frontier, shared candidate lists)"
-    return "staged segments (thread per sample)"
+    return "ray per warp (warp-wide BVH frontier, shared candidate lists)"
 
 
 def config_dict(args):
@@ -464,7 +462,7 @@ def batched_timing(args, dev, stream):
     {256^2, 512^2, 1024^2}, 1-16 spp, majorant tracking. Timed with CUDA events: every scene
     rendered by its own launch in sequence, and all scenes in one persistent launch replayed
     from a CUDA graph with the launch shape the autotuner picked (tuned on a 1-spp copy of the
-    batch). The plain estimator (global majorant, thread per sample) is timed on the first
+    batch). The plain estimator (global majorant 1/unit, ray per warp) is timed on the first
     eight scenes at 1 spp."""
     import torch
     import aarbf
@@ -627,19 +625,29 @@ def series_timing(args, sc, xyzw_pin, radii_pin, tf, dom, rmax, dev):
         return params_for(args, dom, rmax, frame_id=k, spp=1)
 
     out = {"frames": len(frames), "spp": 1}
-    sr = streaming.SeriesRenderer(dev.index or 0, dom, tf, rmax, ppl=args.ppl, alpha_floor=args.alpha_floor)
-    sr.render_series(frames[:2], params, W, H, accum, imgs[:2])  # warm-up (allocations)
-    for overlap in (False, True):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        sr.render_series(frames, params, W, H, accum, imgs, overlap=overlap)
-        torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
-        out["overlapped" if overlap else "sequential"] = {"ms_per_frame": dt / len(frames) * 1e3,
-                                                          "frames_s": len(frames) / dt}
-    sr.close()
+    ref_imgs = None
+    for update in ("build", "refit", "refit_keep_order"):
+        sr = streaming.SeriesRenderer(dev.index or 0, dom, tf, rmax, ppl=args.ppl, alpha_floor=args.alpha_floor,
+                                      update=update)
+        sr.render_series(frames[:2], params, W, H, accum, imgs[:2])  # warm-up (allocations, first builds)
+        for overlap in (False, True):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            sr.render_series(frames, params, W, H, accum, imgs, overlap=overlap)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            key = ("overlapped" if overlap else "sequential") + ("" if update == "build" else "_" + update)
+            out[key] = {"ms_per_frame": dt / len(frames) * 1e3, "frames_s": len(frames) / dt}
+        sr.close()
+        if ref_imgs is None:
+            ref_imgs = [i.clone() for i in imgs]
+        else:
+            out[f"images_identical_{update}"] = all(torch.equal(a, b) for a, b in zip(ref_imgs, imgs))
     out["speedup"] = out["overlapped"]["frames_s"] / out["sequential"]["frames_s"]
-    out["timing"] = "host wall clock around the whole series (uploads, builds and renders of every frame)"
+    out["speedup_refit"] = out["sequential_refit"]["frames_s"] / out["sequential"]["frames_s"]
+    out["timing"] = ("host wall clock around the whole series (uploads, builds or refits and renders of every "
+                     "frame); refit: the frame is sorted along the curve and refits the first build's topology "
+                     "(the reference's update path); refit_keep_order: no sort")
     return out
 
 

@@ -59,8 +59,8 @@ enum {
 
 /* Traversal strategies of the render kernel; every choice gives bit-identical results. */
 enum {
-  AARBF_TRAVERSAL_AUTO = 0,  /* majorant tracking: one warp per ray (cooperative traversal and
-                                sums); otherwise per-thread staged segments */
+  AARBF_TRAVERSAL_AUTO = 0,  /* one warp per ray (cooperative traversal, staged candidate lists
+                                and fixed-point sums) for every estimator */
   AARBF_TRAVERSAL_POINT = 1, /* one BVH point query per tracking step (reference shape) */
   AARBF_TRAVERSAL_THREAD = 2 /* per-thread staged segments for every estimator */
 };
@@ -90,9 +90,10 @@ typedef struct aarbf_params {
   int32_t candidate_cap;    /* staged candidates per ray: 16, 32, 64 or 128 per thread (0 = 32),
                                or 256, 512 or 1024 per warp for the warp kernel (0 = 256);
                                tuning only, results are identical for every value */
-  int32_t stage_bins;       /* majorant tracking: bins staged by the first traversal of a ray
-                               (1..64; 0 = 4 for the warp kernel, 16 per thread; later stagings
-                               double up to 64); tuning only */
+  int32_t stage_bins;       /* bins staged by the first traversal of a ray (1..64; 0 = 4 for the
+                               warp kernel, 16 per thread; later stagings double up to 64); the
+                               bins are bin_length long (16 units when bin_length is 0 and majorant
+                               tracking is off); tuning only */
   uint32_t loop_cap;        /* 0 = the built-in iteration bounds of the device loops (the
                                reference's MAX_DEPTH step budget is not one of them). A positive
                                value lowers every bound to it, so the status path can be
@@ -161,6 +162,20 @@ aarbf_status aarbf_build(aarbf_ctx *ctx, float rbf_radius, uint32_t particles_pe
  * (replaces gprtAccelUpdate, hostCode.cpp:791-794). */
 aarbf_status aarbf_refit(aarbf_ctx *ctx, float rbf_radius, void *stream);
 
+/* A new frame of the same particle count (aarbf_set_particles, radii given iff the build had
+ * them), same radius and transfer functions: the BVH keeps the topology of the last aarbf_build
+ * and is refit to the new frame's leaves, as the reference refits on a frame change
+ * (hostCode.cpp:751-794: the frame upload, GenRBFBounds and gprtAccelUpdate when the radius did
+ * not change). keep_order = 0: the new frame is sorted along the Hilbert curve of the build's
+ * space-time box, as the reference pre-sorts every frame (hostCode.cpp:195-222), and its leaves
+ * refit the old topology; keep_order = 1: the frame's particles keep the previous frame's order
+ * (particle i of every frame is the same particle), so nothing is sorted; aarbf_get_hilbert_keys
+ * then still returns the keys of the last sort. Renders are bit-identical to a full aarbf_build
+ * of the frame in either case (the sums are exact and the traversal only culls). A different
+ * count or storage form returns AARBF_ERR_INVALID_ARGUMENT: call aarbf_build. Synchronises
+ * `stream` once (root box read-back, and the tie check of the sort when keep_order = 0). */
+aarbf_status aarbf_refit_frame(aarbf_ctx *ctx, int keep_order, void *stream);
+
 /* ---- rendering --------------------------------------------------------------------------- */
 
 /* ParticleRBFRayGen (deviceCodeRBF.hlsl:206-336) with the intersection/any-hit programs
@@ -173,10 +188,12 @@ aarbf_status aarbf_render(aarbf_ctx *ctx, const aarbf_params *p, int width, int 
  * (primary [start, termination] and shadow), [1] BVH nodes those segment queries visit, then the
  * kernel's own work: [2] tracking steps, [3] segment stagings, [4] staging overflows, [5] point
  * queries, [6] staged-candidate checks, [7] particle evaluations, [8] node visits while staging,
- * [9] node visits of point queries. The ray-per-warp kernel (majorant tracking with
- * AARBF_TRAVERSAL_AUTO) fills [2..9] with its own work instead: [2] tentative steps, [3] segment
- * stagings, [4] staging overflows, [5] direct (unstaged) bin sums, [6] candidates staged, [7] bins
- * and sub-bins visited, [8] warp traversal iterations, [9] particles tested by the traversals.
+ * [9] node visits of point queries. The ray-per-warp kernels (AARBF_TRAVERSAL_AUTO) fill [2..9]
+ * with their own work instead: [2] tentative steps, [3] segment stagings, [4] staging overflows,
+ * [5] direct (unstaged) bin sums or point queries, [6] candidates staged, [7] bins and sub-bins
+ * visited (majorant tracking), [8] warp traversal iterations, [9] particles tested by the
+ * traversals. Count-mode launches use the timed instances' grid (their larger frames fit fewer
+ * blocks per SM, so they run oversubscribed; work comes from an atomic counter either way).
  * Synchronises `stream`. */
 #define AARBF_COUNT_SLOTS 10
 aarbf_status aarbf_render_count(aarbf_ctx *ctx, const aarbf_params *p, int width, int height,

@@ -168,7 +168,7 @@ def reference_params(aarbf_mod, dom, w, h, **kw):
     return aarbf_mod.RenderParams(**base), r
 
 
-@pytest.mark.parametrize("traversal", [0, 1])
+@pytest.mark.parametrize("traversal", [0, 1, 2])  # one warp per ray / point queries / one thread per ray
 @pytest.mark.parametrize("ppl", [1, 4])
 def test_render_tracking_reference_mode(ctx, orc, aarbf_mod, traversal, ppl):
     xyzw, _ = random_scene(20_000, 11)
@@ -265,7 +265,30 @@ def test_render_marching_native_dense(ctx, orc, aarbf_mod, traversal):
     assert (oi[..., :3] > 0).mean() > 0.01
 
 
-@pytest.mark.parametrize("traversal", [0, 1])
+@pytest.mark.parametrize("traversal", [0, 2])
+@pytest.mark.parametrize("cap,bins", [(256, 0), (1024, 64)])
+def test_render_delta_native_dense(ctx, orc, aarbf_mod, traversal, cap, bins):
+    """the reference's delta tracking (global majorant 1/unit, native density) through dense
+    clusters: the warp tracker's stagings overflow and fall back to shorter runs and direct warp
+    point queries; every buffer depth and first staging length gives the same bits"""
+    from aarbf import scenes
+    sc = scenes.config_clusters(60_000, clusters=8, seed=19)
+    cm, rm, dm = scenes.tf_linear_ramp()
+    dom = orc.domain([sc.xyzw])
+    w, h = 32, 24
+    rp = scenes.native_params(scenes.orbit_camera(), w, h, float(sc.radii.max()), 0.002, 400.0, dom, spp=2,
+                              traversal=traversal, bin_length=0.032)
+    if traversal == 0:
+        rp.candidate_cap, rp.stage_bins = cap, bins
+    scene, *_ = setup_both(ctx, orc, aarbf_mod, sc.xyzw, sc.radii, 4, rp.rbf_radius, tf32=(cm, rm, dm))
+    ga, gi = gpu_render(ctx, rp, w, h)
+    oa, oi = scene.render(orc.params_from(rp), w, h)
+    assert_radiance(gi, oi, "image")
+    assert_radiance(ga, oa, "accum")
+    assert (oi[..., :3] > 0).mean() > 0.01
+
+
+@pytest.mark.parametrize("traversal", [0, 1, 2])
 def test_render_native_mode(ctx, orc, aarbf_mod, traversal):
     from aarbf import scenes
     sc = scenes.config_clusters(30_000, clusters=8, seed=5)
