@@ -1,11 +1,14 @@
 // aarbf -- headless command-line front end, the argparse CLI of the reference's hostCode.cpp
 // (:103-131) on top of the C ABI: --particles PATH, --camera 10 floats, --radius F,
 // --particles-per-leaf U, plus headless options (--out, --frames, --spp, --width, --height,
-// --mode track|march|splat, --taa, --start-frame).
+// --mode track|march|splat, --taa, --start-frame, --rebuild).
 //
 // Pipeline per hostCode.cpp: load the series (or the built-in synthetic one, :147-168), compute
-// the space-time domain over all frames (:183-193), then per frame: upload, build (Hilbert sort,
-// bounds, LBVH), render and optionally resolve TAA, writing <out>_<frame>.pfm.
+// the space-time domain over all frames (:183-193), then per frame: upload, build the BVH on the
+// first frame (Hilbert sort, bounds, LBVH) and refit it on a frame change of the same particle
+// count (the frame sorted along the curve, its leaves refitting the first build's topology, as the
+// reference's gprtAccelUpdate path, :751-794; --rebuild builds every frame instead), render and
+// optionally resolve TAA, writing <out>_<frame>.pfm.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -26,13 +29,15 @@ struct Args {
   int frames = 1, start = 0, spp = 1, width = 1920, height = 1080;
   std::string mode = "track";
   bool taa = false;
+  bool rebuild = false;
 };
 
 void usage() {
   fprintf(stderr,
           "Usage: aarbf [--particles PATH] [--camera px py pz ax ay az ux uy uz fovy] [--radius R]\n"
           "             [--particles-per-leaf N] [--out PREFIX] [--frames N] [--start-frame F]\n"
-          "             [--spp N] [--width W] [--height H] [--mode track|march|splat] [--taa]\n");
+          "             [--spp N] [--width W] [--height H] [--mode track|march|splat] [--taa]\n"
+          "             [--rebuild]\n");
 }
 
 bool parse(int argc, char** argv, Args& a) {
@@ -80,6 +85,8 @@ bool parse(int argc, char** argv, Args& a) {
       a.mode = argv[++i];
     } else if (k == "--taa") {
       a.taa = true;
+    } else if (k == "--rebuild") {
+      a.rebuild = true;
     } else if (k == "-h" || k == "--help") {
       usage();
       exit(0);
@@ -217,10 +224,16 @@ int main(int argc, char** argv) {
   }
   std::vector<float> host(4 * (size_t)a.width * a.height);
   uint32_t frame_id = 0;
+  size_t built_count = 0;
   for (int k = 0; k < a.frames; ++k) {
     auto& f = frames[(size_t)(a.start + k) % frames.size()];
     CHECK(ctx, aarbf_set_particles(ctx, f.data(), f.size() / 4, nullptr, nullptr));
-    CHECK(ctx, aarbf_build(ctx, radius, a.ppl, nullptr));
+    if (k == 0 || a.rebuild || f.size() / 4 != built_count) {
+      CHECK(ctx, aarbf_build(ctx, radius, a.ppl, nullptr));
+      built_count = f.size() / 4;
+    } else {
+      CHECK(ctx, aarbf_refit_frame(ctx, 0, nullptr));
+    }
     p.accum_id = 1;
     p.frame_id = frame_id;
     if (a.mode == "splat") CHECK(ctx, aarbf_render_splat(ctx, &p, a.width, a.height, image, nullptr));

@@ -1121,25 +1121,6 @@ aarbf_status aarbf_set_noise_atlas(aarbf_ctx* ctx, const uint8_t* rgba8, int w, 
   return AARBF_OK;
 }
 
-// Substitute for the missing stbn.png: each 256x256 tile of the 8x16 atlas is an R2
-// low-discrepancy dither (Roberts 2018) offset per tile by the golden ratio, quantised to 8 bits.
-aarbf_status aarbf_generate_noise_atlas(uint8_t* out, int w, int h) {
-  if (!out || w <= 0 || h <= 0) return AARBF_ERR_INVALID_ARGUMENT;
-  const double g = 1.22074408460575947536;  // plastic constant
-  const double a1 = 1.0 / g, a2 = 1.0 / (g * g), phi = 0.61803398874989484820;
-  for (int y = 0; y < h; ++y) {
-    for (int x = 0; x < w; ++x) {
-      int tile = (y / 256) * 8 + (x / 256);
-      double v = 0.5 + a1 * (x % 256) + a2 * (y % 256) + phi * tile;
-      v -= std::floor(v);
-      uint8_t b = (uint8_t)std::min(255.0, std::floor(v * 256.0));
-      uint8_t* p = out + 4 * ((size_t)y * w + x);
-      p[0] = p[1] = p[2] = b;
-      p[3] = 255;
-    }
-  }
-  return AARBF_OK;
-}
 
 aarbf_status aarbf_camera(const float* from, const float* at, const float* up, float cos_fovy, int w, int h,
                           float* pos, float* d00, float* du, float* dv) {

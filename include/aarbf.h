@@ -279,7 +279,10 @@ aarbf_status aarbf_memcpy(aarbf_ctx *ctx, void *dst, const void *src, size_t byt
 aarbf_status aarbf_memset(aarbf_ctx *ctx, void *dst, int value, size_t bytes, void *stream);
 
 /* Blue-noise atlas for the marching mode: RGBA8, 8 x 16 tiles of 256 x 256 (stbn.png layout,
- * hostCode.cpp:337-352). NULL selects a generated substitute (aarbf_generate_noise_atlas). */
+ * hostCode.cpp:337-352). NULL selects a generated substitute (aarbf_generate_noise_atlas: one
+ * void-and-cluster blue-noise tile, frame f's tile offset by f times the golden-ratio conjugate
+ * modulo 1; every tile holds each 8-bit value 256 times; the first call takes a few seconds of
+ * host time, later calls reuse the tile). */
 aarbf_status aarbf_set_noise_atlas(aarbf_ctx *ctx, const uint8_t *rgba8, int width, int height);
 aarbf_status aarbf_generate_noise_atlas(uint8_t *rgba8_out, int width, int height);
 

@@ -108,3 +108,32 @@ def test_reference_synthetic_dataset():
     assert len(fr) == 3 and fr[0].shape == (1000, 4)
     # attribute = y / 10 and frame 0 scale = sin(0) + 1.5 (hostCode.cpp:157-163)
     assert np.isclose(fr[0][999, 3], 0.9) and np.isclose(fr[0][0, 0], 1.5 * -0.5)
+
+
+def test_noise_atlas_is_spatiotemporal_blue_noise(aarbf_mod):
+    """aarbf_generate_noise_atlas (host code, no GPU): 8 x 16 tiles of 256 x 256 in the reference's
+    stbn.png layout (hostCode.cpp:337-352); each tile holds every 8-bit value exactly 256 times;
+    tile 0 is void-and-cluster blue noise (almost no energy at low spatial frequencies, where white
+    noise keeps its area share), the other frames are its golden-ratio shifts (still far below
+    white noise at low frequencies), and a texel's values over successive frames advance by the
+    golden-ratio conjugate modulo 1."""
+    a = aarbf_mod.generate_noise_atlas()
+    assert a.shape == (4096, 2048, 4) and (a[..., 3] == 255).all()
+    assert np.array_equal(a, aarbf_mod.generate_noise_atlas())  # deterministic
+    k = np.fft.fftfreq(256) * 256
+    low = np.sqrt(k[:, None] ** 2 + k[None, :] ** 2) < 32  # 4.9 % of the spectrum
+
+    def low_share(t):
+        f = np.abs(np.fft.fft2(t - t.mean())) ** 2
+        return f[low].sum() / f.sum()
+
+    tiles = [a[256 * (f // 8):256 * (f // 8 + 1), 256 * (f % 8):256 * (f % 8 + 1), 0].astype(np.float64)
+             for f in range(128)]
+    for f in (0, 1, 37, 127):
+        assert (np.bincount(tiles[f].astype(np.int64).ravel(), minlength=256) == 256).all()
+    assert low_share(tiles[0]) < 1e-3
+    assert max(low_share(tiles[f]) for f in (1, 2, 37, 127)) < 1e-2
+    white = np.random.default_rng(0).integers(0, 256, (256, 256)).astype(np.float64)
+    assert low_share(white) > 0.03
+    step = (tiles[1].astype(np.int64) - tiles[0].astype(np.int64)) % 256
+    assert np.isin(step, [157, 158, 159]).all()  # 0.618 x 256 = 158.2
