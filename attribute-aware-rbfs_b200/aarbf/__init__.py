@@ -66,7 +66,7 @@ EXPORTED_SYMBOLS = (
     "aarbf_memcpy", "aarbf_memset", "aarbf_render_count", "aarbf_set_opacity_floor",
     "aarbf_hilbert_sort_noalloc", "aarbf_set_kernel_timing", "aarbf_get_kernel_times",
     "aarbf_render_diff_forward", "aarbf_render_diff_backward", "aarbf_batch_create", "aarbf_batch_render",
-    "aarbf_batch_destroy", "aarbf_batch_last_error", "aarbf_set_storage",
+    "aarbf_batch_destroy", "aarbf_batch_last_error", "aarbf_set_storage", "aarbf_batch_set_shape",
 )
 
 
@@ -143,6 +143,7 @@ def _load():
         "aarbf_set_storage": [P, i32],
         "aarbf_batch_create": [ctypes.POINTER(P), P, ctypes.POINTER(Params), i32, P, P, P, P],
         "aarbf_batch_render": [P, i32, P],
+        "aarbf_batch_set_shape": [P, i32, i32],
         "aarbf_batch_destroy": [P],
         "aarbf_render_diff_forward": [P, ctypes.POINTER(Params), i32, i32, i32, P, P],
         "aarbf_render_diff_backward": [P, ctypes.POINTER(Params), i32, i32, i32, P, P, P, P, P, P],
@@ -587,6 +588,12 @@ class Batch:
 
     def render(self, candidate_cap: int = 0, stream=None):
         st = self._lib.aarbf_batch_render(self._h, int(candidate_cap), _stream_ptr(stream))
+        if st != 0:
+            raise AarbfError(st, self._lib.aarbf_batch_last_error(self._h).decode())
+
+    def set_shape(self, blocks_per_sm: int = 0, sample_major: bool = False):
+        """aarbf_batch_set_shape: resident blocks per SM (0 = occupancy limit) and work-item order."""
+        st = self._lib.aarbf_batch_set_shape(self._h, int(blocks_per_sm), int(bool(sample_major)))
         if st != 0:
             raise AarbfError(st, self._lib.aarbf_batch_last_error(self._h).decode())
 

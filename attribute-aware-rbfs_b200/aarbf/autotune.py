@@ -1,10 +1,18 @@
 """Launch-shape autotuner of the batched renderer.
 
-The staging-buffer depth of the ray-per-warp kernel (candidate_cap 256, 512 or 1024) and the
-number of majorant bins its first staging covers (stage_bins) change only speed, never results.
-The best pair depends on the scenes (particle density along the rays, resolution, spp), so the
-tuner times every pair on the batch itself with CUDA events and keeps the fastest, cached per
-batch signature.
+Every knob changes only speed, never results:
+  - candidate_cap: staging-buffer depth of the ray-per-warp kernel (256, 512 or 1024 candidates);
+  - stage_bins: majorant bins covered by a ray's first staging (2, 4 or 8; later stagings double);
+  - blocks_per_sm: resident blocks of four warps per SM (6, 7 or the occupancy limit of 8), the
+    block-level shape of the persistent launch;
+  - sample_major: the ray order -- the work items of a batch run tile by tile with a tile's
+    samples in sequence (rays of one 8 x 4 pixel tile together), or sample by sample over all
+    tiles;
+  - scene order: scenes are placed longest first (by their own timed 1-spp proxy render scaled
+    by spp), so the persistent launch ends on short work instead of one long scene.
+The best setting depends on the scenes (particle density along the rays, resolution, spp), so
+the tuner times the batch itself with CUDA events, one knob after the other (the pair of staging
+knobs jointly), and caches the result per batch signature.
 """
 from __future__ import annotations
 
@@ -12,6 +20,8 @@ import copy
 
 CAPS = (256, 512, 1024)
 STAGE_BINS = (2, 4, 8)
+BLOCKS_PER_SM = (6, 7, 0)
+SAMPLE_MAJOR = (False, True)
 
 _cache: dict = {}
 
@@ -20,8 +30,33 @@ def signature(contexts, params, sizes) -> tuple:
     return tuple((id(c), int(p.spp), int(w), int(h)) for c, p, (w, h) in zip(contexts, params, sizes))
 
 
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def scene_order(contexts, params, sizes, accums, images, stream=None):
+    """indices of the scenes, longest first: each scene's 1-spp render timed on its own, times its spp"""
+    import torch
+    st = stream or torch.cuda.current_stream()
+    cost = []
+    for i, (c, p, (w, h), a, im) in enumerate(zip(contexts, params, sizes, accums, images)):
+        q = copy.copy(p)
+        q.spp = 1
+        c.render(q, w, h, a, im, stream=st.cuda_stream)
+        e0, e1 = _events()
+        e0.record(st)
+        c.render(q, w, h, a, im, stream=st.cuda_stream)
+        e1.record(st)
+        torch.cuda.synchronize()
+        cost.append(e0.elapsed_time(e1) * max(int(p.spp), 1))
+    return sorted(range(len(cost)), key=lambda i: -cost[i])
+
+
 def tune_batch(contexts, params, sizes, accums, images, stream=None, reps: int = 1):
-    """(candidate_cap, stage_bins, {(cap, bins): ms}) of the fastest batched launch."""
+    """(candidate_cap, stage_bins, {(cap, bins): ms}) of the fastest batched launch (tuned on these
+    parameters; the caller usually passes 1-spp proxies of its scenes). The blocks-per-SM and
+    ray-order choices are in tune_shape."""
     import torch
 
     from . import Batch
@@ -39,7 +74,7 @@ def tune_batch(contexts, params, sizes, accums, images, stream=None, reps: int =
         b = Batch(contexts, ps, sizes, accums, images)
         for cap in CAPS:
             b.render(cap, st)  # warm-up
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0, e1 = _events()
             e0.record(st)
             for _ in range(reps):
                 b.render(cap, st)
@@ -50,3 +85,25 @@ def tune_batch(contexts, params, sizes, accums, images, stream=None, reps: int =
     best = min(times, key=times.get)
     _cache[key] = (best[0], best[1], times)
     return _cache[key]
+
+
+def tune_shape(batch, candidate_cap, stream=None, reps: int = 1):
+    """(blocks_per_sm, sample_major, {(blocks_per_sm, sample_major): ms}) of the fastest launch
+    shape of an existing Batch; the batch is left set to it."""
+    import torch
+    st = stream or torch.cuda.current_stream()
+    times = {}
+    for bps in BLOCKS_PER_SM:
+        for sm in SAMPLE_MAJOR:
+            batch.set_shape(bps, sm)
+            batch.render(candidate_cap, st)
+            e0, e1 = _events()
+            e0.record(st)
+            for _ in range(reps):
+                batch.render(candidate_cap, st)
+            e1.record(st)
+            torch.cuda.synchronize()
+            times[(bps, sm)] = e0.elapsed_time(e1) / reps
+    best = min(times, key=times.get)
+    batch.set_shape(*best)
+    return best[0], best[1], times

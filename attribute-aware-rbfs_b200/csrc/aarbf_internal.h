@@ -191,6 +191,8 @@ struct BatchArgs {
   unsigned long long* work_counter;
   uint32_t* warp_stacks;
   bool fp16;                     // every scene is in the FP16 storage form
+  int blocks_per_sm;             // resident blocks per SM (0 = the occupancy limit)
+  int sample_major;              // work items sample by sample (1) or tile by tile (0)
 };
 inline cudaError_t launch_render_batched(const BatchArgs& B, cudaStream_t st) {
   return B.fp16 ? r16::launch_render_batched(B, st) : r32::launch_render_batched(B, st);

@@ -783,8 +783,21 @@ struct aarbf_batch {
   DevBuf dev;           // launch blocks, item and pixel prefix sums, work counter
   uint32_t* warp_stacks = nullptr;
   bool fp16 = false;
+  int blocks_per_sm = 0;  // launch shape (aarbf_batch_set_shape)
+  int sample_major = 0;
   std::string last_error;
 };
+
+aarbf_status aarbf_batch_set_shape(aarbf_batch* b, int blocks_per_sm, int sample_major) {
+  if (!b) return AARBF_ERR_INVALID_ARGUMENT;
+  if (blocks_per_sm < 0 || blocks_per_sm > 64 || (sample_major != 0 && sample_major != 1)) {
+    b->last_error = "blocks_per_sm must lie in 0..64 and sample_major be 0 or 1";
+    return AARBF_ERR_INVALID_ARGUMENT;
+  }
+  b->blocks_per_sm = blocks_per_sm;
+  b->sample_major = sample_major;
+  return AARBF_OK;
+}
 
 aarbf_status aarbf_batch_create(aarbf_batch** out, aarbf_ctx* const* ctxs, const aarbf_params* params, int nscenes,
                                 const int* widths, const int* heights, float* const* accums, float* const* images) {
@@ -865,6 +878,8 @@ aarbf_status aarbf_batch_render(aarbf_batch* b, int candidate_cap, void* stream)
   B.work_counter = reinterpret_cast<unsigned long long*>(base + off_ctr);
   B.warp_stacks = b->warp_stacks;
   B.fp16 = b->fp16;
+  B.blocks_per_sm = b->blocks_per_sm;
+  B.sample_major = b->sample_major;
   cudaError_t e = launch_render_batched(B, (cudaStream_t)stream);
   if (e != cudaSuccess) {
     b->last_error = std::string("batch render: ") + cudaGetErrorString(e);

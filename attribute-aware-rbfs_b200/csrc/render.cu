@@ -89,6 +89,18 @@ __device__ __forceinline__ void eval_particle(const SceneView& s, uint32_t i, fl
   acc.a3 += fix40(rho * w.w);
 }
 
+// the density part of eval_particle only: the hot loops need the colour sums only at a collision
+__device__ __forceinline__ void eval_density(const SceneView& s, uint32_t i, float3 x, int& count, long long& a0) {
+  float4 r = part_rec(s, i);
+  float dx = r.x - x.x, dy = r.y - x.y, dz = r.z - x.z;
+  float dist = sqrtf((dx * dx + dy * dy) + dz * dz);
+  if (!(dist < r.w)) return;
+  float q = (dist * 3.0f) / r.w;
+  float rho = dexp(-0.5f * (q * q));
+  count += 1;
+  a0 += fix40(rho * part_a3(s, i));
+}
+
 __device__ __forceinline__ void eval_leaf(const SceneView& s, uint32_t leaf, float3 x, Sample& acc) {
   uint64_t b = (uint64_t)leaf * s.ppl;
   uint64_t e = b + s.ppl;
@@ -1020,6 +1032,26 @@ struct WarpStager {
     warp_sum_sample(acc);
   }
 
+  // the density sum at step point x (t on the ray) over bin kbin's candidates, warp-reduced;
+  // any: some particle holds x. The colour sums are left to sample() (once per collision).
+  __device__ long long sample_density(const SceneView& s, int kbin, float t, float3 x, bool& any) const {
+    int first, last;
+    range(kbin, first, last);
+    if (first >= last) {  // no candidate in this bin (warp-uniform)
+      any = false;
+      return 0;
+    }
+    long long a0 = 0;
+    int count = 0;
+    for (int p = first + (int)(threadIdx.x & 31u); p < last; p += 32) {
+      int j = slot(p);
+      if (t < buf->lo[j] || t > buf->hi[j]) continue;
+      eval_density(s, buf->idx[j], x, count, a0);
+    }
+    any = __any_sync(kFull, count > 0);
+    return any ? warp_sum(a0) : 0;
+  }
+
   // first bin >= k of the staged segment whose list is not empty (kseg + nbins if none)
   __device__ int next_nonempty(int k) const {
     if (!lists) return k;
@@ -1178,11 +1210,18 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
           if (t >= hi || t >= ray.tmax) break;
           float3 x = make_float3(ray.o.x + t * ray.d.x, ray.o.y + t * ray.d.y, ray.o.z + t * ray.d.z);
           Sample smp;
-          if (direct) smp = warp_point<CAPW>(L.s, x, buf, stk, L.status, ctr);
-          else st.sample(L.s, k, t, x, smp);
-          float D = (float)smp.a0 * kFixInv;
+          long long a0;
+          if (direct) {
+            smp = warp_point<CAPW>(L.s, x, buf, stk, L.status, ctr);
+            a0 = smp.a0;
+          } else {
+            bool any;
+            a0 = st.sample_density(L.s, k, t, x, any);
+          }
+          float D = (float)a0 * kFixInv;
           float sigma = D * scale;
           if (lcg_f(tr.rng) < sigma / M) {
+            if (!direct) st.sample(L.s, k, t, x, smp);  // the colour sums of the collision
             float3 c = sample_color(L, smp, D);
             tr.albedo = make_float4(c.x, c.y, c.z, 1.0f);
             tr.t = t;
@@ -1268,12 +1307,20 @@ __device__ __forceinline__ void track_delta_warp_body(const RenderLaunch& L, Tra
     }
     const float3 x = make_float3(ray.o.x + t * ray.d.x, ray.o.y + t * ray.d.y, ray.o.z + t * ray.d.z);
     Sample smp;
-    if (direct) smp = warp_point<CAPW>(L.s, x, buf, stk, L.status, ctr);
-    else st.sample(L.s, kb, t, x, smp);
-    if (smp.count == 0) continue;
-    const float D = (float)smp.a0 * kFixInv;
+    long long a0;
+    bool any;
+    if (direct) {
+      smp = warp_point<CAPW>(L.s, x, buf, stk, L.status, ctr);
+      a0 = smp.a0;
+      any = smp.count > 0;
+    } else {
+      a0 = st.sample_density(L.s, kb, t, x, any);
+    }
+    if (!any) continue;
+    const float D = (float)a0 * kFixInv;
     const float density = sample_density(L, D);
     if (lcg_f(tr.rng) < density / 1.0f) {
+      if (!direct) st.sample(L.s, kb, t, x, smp);  // the colour sums of the collision
       const float3 c = sample_color(L, smp, D);
       tr.albedo = make_float4(c.x, c.y, c.z, 1.0f);
       return;
@@ -1376,10 +1423,10 @@ __device__ __forceinline__ void track_march_warp_body(const RenderLaunch& L, Tra
     const float3 x = make_float3(ray.o.x + tj * ray.d.x, ray.o.y + tj * ray.d.y, ray.o.z + tj * ray.d.z);
     Sample smp;
     sample_clear(smp);
-    if (!direct) {
+    if (!direct) {  // each lane its step's density; the colour sums only for the stopping step
       for (int c = 0; c < n; ++c) {
         const bool in = active && tj < ray.tmax && tj >= buf->lo[c] && tj <= buf->hi[c];
-        if (in) eval_particle(s, buf->idx[c], x, smp);
+        if (in) eval_density(s, buf->idx[c], x, smp.count, smp.a0);
       }
     } else {
       const float3 x0 = make_float3(__shfl_sync(kFull, x.x, 0), __shfl_sync(kFull, x.y, 0), __shfl_sync(kFull, x.z, 0));
@@ -1432,7 +1479,14 @@ __device__ __forceinline__ void track_march_warp_body(const RenderLaunch& L, Tra
         tr.albedo.w = alpha;
       } else {
         float3 c = make_float3(0.0f, 0.0f, 0.0f);
-        if ((int)lane == stop) c = sample_color(L, smp, D);
+        if ((int)lane == stop) {
+          if (!direct) {  // the stopping step's colour sums over the same candidates
+            sample_clear(smp);
+            for (int q = 0; q < n; ++q)
+              if (tj >= buf->lo[q] && tj <= buf->hi[q]) eval_particle(s, buf->idx[q], x, smp);
+          }
+          c = sample_color(L, smp, D);
+        }
         tr.albedo = make_float4(__shfl_sync(kFull, c.x, stop), __shfl_sync(kFull, c.y, stop),
                                 __shfl_sync(kFull, c.z, stop), 1.0f);
       }
@@ -1467,10 +1521,12 @@ __device__ __forceinline__ uint32_t warp_items(const RenderLaunch& L) {
 enum { kWarpMajorant = 0, kWarpMarch = 1, kWarpDelta = 2 };
 
 // one work item of the ray-per-warp kernel (all lanes of the warp); COUNT: the count-mode instance
-// (render_count), so the timed instance carries no accounting code
+// (render_count), so the timed instance carries no accounting code. sample_major: items run over
+// every 8 x 4 tile for one sample before the next sample (else a tile's samples follow each
+// other); the image is the same either way
 template <int CAPW, int MODE, bool COUNT>
 __device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t item, WarpBuf<CAPW>* buf,
-                                                 uint32_t* stk) {
+                                                 uint32_t* stk, bool sample_major = false) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t tiles_x = (uint32_t)(L.width + 7) / 8u;
   const uint32_t spp = L.spp ? L.spp : 1u;
@@ -1478,6 +1534,11 @@ __device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t
   const bool cost = (L.flags & kFlagCostImage) != 0;
   uint32_t group = item >> 5, in = item & 31u;
   uint32_t tile = group / spp, k = group % spp;
+  if (sample_major) {
+    const uint32_t ntiles = tiles_x * ((uint32_t)(L.height + 3) / 4u);
+    k = group / ntiles;
+    tile = group % ntiles;
+  }
   const int px = (int)((tile % tiles_x) * 8u + (in & 7u));
   const int py = (int)((tile / tiles_x) * 4u + (in >> 3));
   if (px >= L.width || py >= L.height) return;
@@ -1518,7 +1579,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks) k_render_
 template <int CAPW>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks)
     k_render_warp_batched(const RenderLaunch* __restrict__ Ls, const uint64_t* __restrict__ item_ofs, int nscenes,
-                          unsigned long long* work_counter, uint32_t* warp_stacks) {
+                          unsigned long long* work_counter, uint32_t* warp_stacks, int sample_major) {
   extern __shared__ __align__(16) char smem[];
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
   WarpBuf<CAPW>* buf = reinterpret_cast<WarpBuf<CAPW>*>(smem) + wib;
@@ -1535,7 +1596,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks)
       if (item_ofs[mid] <= item) lo = mid;
       else hi = mid;
     }
-    render_warp_item<CAPW, kWarpMajorant, false>(Ls[lo], (uint32_t)(item - item_ofs[lo]), buf, stk);
+    render_warp_item<CAPW, kWarpMajorant, false>(Ls[lo], (uint32_t)(item - item_ofs[lo]), buf, stk,
+                                                 sample_major != 0);
   }
 }
 
@@ -1736,10 +1798,17 @@ cudaError_t launch_warp_batched(const BatchArgs& B, cudaStream_t st) {
   int blocks = 0;
   cudaError_t e = warp_grid<CAPW>(&blocks);
   if (e != cudaSuccess) return e;
+  if (B.blocks_per_sm > 0) {  // fewer resident blocks than the occupancy limit
+    int dev = 0, sms = 0;
+    e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    if (sms * B.blocks_per_sm < blocks) blocks = sms * B.blocks_per_sm;
+  }
   e = cudaMemsetAsync(B.work_counter, 0, sizeof(unsigned long long), st);
   if (e != cudaSuccess) return e;
   k_render_warp_batched<CAPW><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(
-      B.launches, B.item_ofs, B.nscenes, B.work_counter, B.warp_stacks);
+      B.launches, B.item_ofs, B.nscenes, B.work_counter, B.warp_stacks, B.sample_major);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (B.total_pixels)

@@ -517,13 +517,24 @@ def batched_timing(args, dev, stream):
         q = copy.copy(p)
         q.spp = 1
         proxy.append(q)
-    cap, bins, table = autotune.tune_batch(ctxs, proxy, sizes, accs, imgs, stream)
+    order = autotune.scene_order(ctxs, params, sizes, accs, imgs, stream)  # longest first
+    o = lambda seq: [seq[i] for i in order]  # noqa: E731
+    cap, bins, table = autotune.tune_batch(o(ctxs), o(proxy), o(sizes), o(accs), o(imgs), stream)
     tuned = []
-    for p in params:
+    for p in o(params):
         q = copy.copy(p)
         q.stage_bins = bins
         tuned.append(q)
-    b = aarbf.Batch(ctxs, tuned, sizes, accs, imgs)
+    proxy_tuned = []
+    for p in o(proxy):
+        q = copy.copy(p)
+        q.stage_bins = bins
+        proxy_tuned.append(q)
+    pb = aarbf.Batch(o(ctxs), proxy_tuned, o(sizes), o(accs), o(imgs))
+    bps, smaj, shape_table = autotune.tune_shape(pb, cap, stream)
+    pb.close()
+    b = aarbf.Batch(o(ctxs), tuned, o(sizes), o(accs), o(imgs))
+    b.set_shape(bps, smaj)
     with torch.cuda.stream(stream):
         b.render(cap, stream)
         torch.cuda.synchronize()
@@ -573,8 +584,11 @@ def batched_timing(args, dev, stream):
             "sequential_ms": t_seq, "sequential_mrays_s": rays / t_seq / 1e3,
             "batched_direct_ms": t_direct, "batched_graph_ms": t_graph, "batched_mrays_s": rays / t_graph / 1e3,
             "speedup_vs_sequential": t_seq / t_graph, "images_identical": bool(same),
-            "autotuned": {"candidate_cap": cap, "stage_bins": bins,
-                          "proxy_ms": {f"{k[0]}/{k[1]}": round(v, 3) for k, v in table.items()}},
+            "autotuned": {"candidate_cap": cap, "stage_bins": bins, "blocks_per_sm": bps or "occupancy limit",
+                          "ray_order": "sample-major" if smaj else "tile-major",
+                          "scene_order": "longest first (1-spp proxy time x spp)",
+                          "proxy_ms": {f"{k[0]}/{k[1]}": round(v, 3) for k, v in table.items()},
+                          "shape_proxy_ms": {f"{k[0]}/{int(k[1])}": round(v, 3) for k, v in shape_table.items()}},
             "plain_estimator_mrays_s": pr / t_plain / 1e3, "plain_sample": "first 8 scenes, 1 spp",
             "speedup_vs_plain": (rays / t_graph) / (pr / t_plain)}
 

@@ -232,6 +232,11 @@ aarbf_status aarbf_batch_create(aarbf_batch **out, aarbf_ctx *const *ctxs, const
                                 int nscenes, const int *widths, const int *heights,
                                 float *const *accums, float *const *images);
 aarbf_status aarbf_batch_render(aarbf_batch *batch, int candidate_cap, void *stream);
+/* Launch shape of the next aarbf_batch_render calls (tuning only: results are identical for every
+ * shape). blocks_per_sm: resident blocks of four warps per SM (0 = as many as fit; 1..64 caps the
+ * grid); sample_major: 1 hands out the work items sample by sample over all 8 x 4 pixel tiles,
+ * 0 (default) tile by tile with a tile's samples in sequence. */
+aarbf_status aarbf_batch_set_shape(aarbf_batch *batch, int blocks_per_sm, int sample_major);
 aarbf_status aarbf_batch_destroy(aarbf_batch *batch);
 const char *aarbf_batch_last_error(const aarbf_batch *batch);
 

@@ -50,14 +50,18 @@ def test_batched_matches_single_renders(aarbf_mod, orc):
     imgs = [torch.zeros_like(a) for a in accs]
     b = aarbf_mod.Batch([c for c, _, _, _ in items], [p for _, p, _, _ in items], [s for _, _, s, _ in items], accs,
                         imgs)
-    for cap in (0, 512, 1024):
+    for cap, bps, smaj in ((0, 0, False), (512, 6, True), (1024, 7, False), (256, 1, True)):
         for a in accs:
             a.zero_()
+        b.set_shape(bps, smaj)  # launch shape: speed only, the same bits
         b.render(cap)
         torch.cuda.synchronize()
         for (ra, ri), a, i in zip(ref, accs, imgs):
             assert np.array_equal(a.cpu().numpy().view(np.uint32), ra.view(np.uint32))
             assert np.array_equal(i.cpu().numpy().view(np.uint32), ri.view(np.uint32))
+    with pytest.raises(aarbf_mod.AarbfError):
+        b.set_shape(-1, False)
+    b.set_shape(0, False)
     # the same launch replayed from a CUDA graph
     st = torch.cuda.Stream()
     with torch.cuda.stream(st):
