@@ -635,10 +635,12 @@ __device__ void track_majorant(const RenderLaunch& L, Tracker& tr, const Ray& ra
       }
     }
     // [b0, b1), split in halves (front first) while majorant * length > kSplitSteps
+    // [b0, b1) and its halves: path bit l set = the interval at level l + 1 is the upper half;
+    // a pending upper half is replayed from [b0, b1) by the same midpoint operations, so its
+    // floats are those a stack of pending intervals would hold
     float lo = b0, hi = b1;
-    int depth = 0, np = 0;
-    float pend_hi[kSplitDepth];
-    int pend_depth[kSplitDepth];
+    int depth = 0;
+    uint32_t path = 0;
     for (;;) {
       long long acc = 0;
       if (direct) {
@@ -653,9 +655,6 @@ __device__ void track_majorant(const RenderLaunch& L, Tracker& tr, const Ray& ra
       if (M > 0.0f) {
         float mid = lo + 0.5f * (hi - lo);
         if (M * (hi - lo) > kSplitSteps && depth < kSplitDepth && mid > lo && mid < hi) {
-          pend_hi[np] = hi;
-          pend_depth[np] = depth + 1;
-          ++np;
           hi = mid;
           depth += 1;
           continue;
@@ -688,11 +687,18 @@ __device__ void track_majorant(const RenderLaunch& L, Tracker& tr, const Ray& ra
           }
         }
       }
-      if (np == 0) break;
-      lo = hi;
-      --np;
-      hi = pend_hi[np];
-      depth = pend_depth[np];
+      const uint32_t pending = ~path & ((1u << depth) - 1u);  // lower halves whose upper half waits
+      if (!pending) break;
+      const int d = 31 - __clz(pending);
+      path = (path | (1u << d)) & ((2u << d) - 1u);
+      depth = d + 1;
+      lo = b0;
+      hi = b1;
+      for (int l = 0; l < depth; ++l) {
+        const float m = lo + 0.5f * (hi - lo);
+        if ((path >> l) & 1u) lo = m;
+        else hi = m;
+      }
     }
     k += 1;
     t = b1;
@@ -899,31 +905,18 @@ struct WarpStager {
     wctr(ctr, kWcStages, 1);
     const float eps = s.eps;
     const float ts = t0 + (float)k * Lb, te = t0 + (float)(k + nb) * Lb;
+    SegSlab slab;
+    slab.init(ray.o, inv, eps, ts, te);
     int n = 0;
     bool ok = warp_traverse(
         s, stk, buf->leaves, status,
-        [&](float lx, float ly, float lz, float hx, float hy, float hz) {
-          return seg_box(lx, ly, lz, hx, hy, hz, ray.o, inv, ts, te, eps);
-        },
+        [&](float lx, float ly, float lz, float hx, float hy, float hz) { return slab.hit(lx, ly, lz, hx, hy, hz); },
         [&](bool v, uint32_t i) -> bool {
           bool keep = false;
           float a = 0.0f, b = 0.0f;
           if (v) {
-            float4 r = part_rec(s, i);
-            if (r.w > 0.0f) {
-              float vx = r.x - ray.o.x, vy = r.y - ray.o.y, vz = r.z - ray.o.z;
-              float tc = (vx * ray.d.x + vy * ray.d.y) + vz * ray.d.z;
-              float wx = vx - tc * ray.d.x, wy = vy - tc * ray.d.y, wz = vz - tc * ray.d.z;
-              float h2 = (wx * wx + wy * wy) + wz * wz;
-              float R = r.w * (1.0f + 0x1p-10f) + eps;
-              float R2 = R * R;
-              if (!(h2 > R2)) {
-                float half = sqrtf(R2 - h2) + eps;
-                a = tc - half;
-                b = tc + half;
-                keep = !(b < ts || a > te);
-              }
-            }
+            const float4 r = part_rec(s, i);
+            if (r.w > 0.0f && sphere_span(r, ray.o, ray.d, eps, a, b)) keep = !(b < ts || a > te);
           }
           const uint32_t m = __ballot_sync(kFull, keep);
           const int cnt = __popc(m);
@@ -1072,12 +1065,11 @@ __device__ __noinline__ long long warp_bin_sum_direct(const SceneView& s, const 
                                                       unsigned long long* ctr) {
   (void)buf;
   long long acc = 0;
-  const float eps = s.eps;
+  SegSlab slab;
+  slab.init(ray.o, inv, s.eps, lo, hi);
   warp_traverse(
       s, stk, warp_buf<CAPW>()->leaves, status,
-      [&](float lx, float ly, float lz, float hx, float hy, float hz) {
-        return seg_box(lx, ly, lz, hx, hy, hz, ray.o, inv, lo, hi, eps);
-      },
+      [&](float lx, float ly, float lz, float hx, float hy, float hz) { return slab.hit(lx, ly, lz, hx, hy, hz); },
       [&](bool v, uint32_t i) -> bool {
         if (v) acc += fix40(bin_contrib(s, ray, i, lo, hi));
         return true;
@@ -1177,10 +1169,12 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
         continue;
       }
     }
+    // [b0, b1) and its halves: path bit l set = the interval at level l + 1 is the upper half;
+    // a pending upper half is replayed from [b0, b1) by the same midpoint operations, so its
+    // floats are those a stack of pending intervals would hold
     float lo = b0, hi = b1;
-    int depth = 0, np = 0;
-    float pend_hi[kSplitDepth];
-    int pend_depth[kSplitDepth];
+    int depth = 0;
+    uint32_t path = 0;
     for (;;) {
       wctr(ctr, kWcBins, 1);
       long long acc = direct ? warp_bin_sum_direct<CAPW>(L.s, ray, st.inv, lo, hi, buf, stk, L.status, ctr)
@@ -1189,9 +1183,6 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
       if (M > 0.0f) {
         float mid = lo + 0.5f * (hi - lo);
         if (M * (hi - lo) > kSplitSteps && depth < kSplitDepth && mid > lo && mid < hi) {
-          pend_hi[np] = hi;
-          pend_depth[np] = depth + 1;
-          ++np;
           hi = mid;
           depth += 1;
           continue;
@@ -1229,11 +1220,18 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
           }
         }
       }
-      if (np == 0) break;
-      lo = hi;
-      --np;
-      hi = pend_hi[np];
-      depth = pend_depth[np];
+      const uint32_t pending = ~path & ((1u << depth) - 1u);  // lower halves whose upper half waits
+      if (!pending) break;
+      const int d = 31 - __clz(pending);
+      path = (path | (1u << d)) & ((2u << d) - 1u);
+      depth = d + 1;
+      lo = b0;
+      hi = b1;
+      for (int l = 0; l < depth; ++l) {
+        const float m = lo + 0.5f * (hi - lo);
+        if ((path >> l) & 1u) lo = m;
+        else hi = m;
+      }
     }
     k += 1;
     t = b1;
@@ -1346,30 +1344,18 @@ __device__ bool stage_segment(const SceneView& s, const Ray& ray, float3 inv, fl
                               uint32_t* stk, uint32_t* status, int& n) {
   const uint32_t lt = lane_lt_mask();
   const float eps = s.eps;
+  SegSlab slab;
+  slab.init(ray.o, inv, eps, ta, tb);
   n = 0;
   const bool ok = warp_traverse(
       s, stk, buf->leaves, status,
-      [&](float lx, float ly, float lz, float hx, float hy, float hz) {
-        return seg_box(lx, ly, lz, hx, hy, hz, ray.o, inv, ta, tb, eps);
-      },
+      [&](float lx, float ly, float lz, float hx, float hy, float hz) { return slab.hit(lx, ly, lz, hx, hy, hz); },
       [&](bool v, uint32_t i) -> bool {
         bool keep = false;
         float a = 0.0f, b = 0.0f;
         if (v) {
-          float4 r = part_rec(s, i);
-          if (r.w > 0.0f) {
-            float vx = r.x - ray.o.x, vy = r.y - ray.o.y, vz = r.z - ray.o.z;
-            float tc = (vx * ray.d.x + vy * ray.d.y) + vz * ray.d.z;
-            float wx = vx - tc * ray.d.x, wy = vy - tc * ray.d.y, wz = vz - tc * ray.d.z;
-            float h2 = (wx * wx + wy * wy) + wz * wz;
-            float R = r.w * (1.0f + 0x1p-10f) + eps;
-            if (!(h2 > R * R)) {
-              float half = sqrtf(R * R - h2) + eps;
-              a = tc - half;
-              b = tc + half;
-              keep = !(b < ta || a > tb);
-            }
-          }
+          const float4 r = part_rec(s, i);
+          if (r.w > 0.0f && sphere_span(r, ray.o, ray.d, eps, a, b)) keep = !(b < ta || a > tb);
         }
         const uint32_t m = __ballot_sync(kFull, keep);
         const int cnt = __popc(m);

@@ -26,6 +26,49 @@ __device__ __forceinline__ bool seg_box(float lx, float ly, float lz, float hx, 
   return tn <= tf;
 }
 
+// The same test with the per-ray terms folded so each slab end is one fused multiply-add:
+// (l - eps - o) inv = l inv + clo, (h + eps - o) inv = h inv + chi. It only culls: its slab ends
+// differ from seg_box's by a few ulps of |o inv|, far inside the eps slack (eps >= 2^-18 of every
+// coordinate and of the camera position). inv is clamped to +-1e30 so an axis-parallel ray meets
+// no inf - inf.
+struct SegSlab {
+  float3 inv, clo, chi;
+  float t0, t1;
+  __device__ __forceinline__ void init(float3 o, float3 inv_ray, float eps, float a, float b) {
+    inv = make_float3(fminf(fmaxf(inv_ray.x, -1e30f), 1e30f), fminf(fmaxf(inv_ray.y, -1e30f), 1e30f),
+                      fminf(fmaxf(inv_ray.z, -1e30f), 1e30f));
+    clo = make_float3(-(o.x + eps) * inv.x, -(o.y + eps) * inv.y, -(o.z + eps) * inv.z);
+    chi = make_float3((eps - o.x) * inv.x, (eps - o.y) * inv.y, (eps - o.z) * inv.z);
+    t0 = a;
+    t1 = b;
+  }
+  __device__ __forceinline__ bool hit(float lx, float ly, float lz, float hx, float hy, float hz) const {
+    const float ax = fmaf(lx, inv.x, clo.x), bx = fmaf(hx, inv.x, chi.x);
+    const float ay = fmaf(ly, inv.y, clo.y), by = fmaf(hy, inv.y, chi.y);
+    const float az = fmaf(lz, inv.z, clo.z), bz = fmaf(hz, inv.z, chi.z);
+    const float tn = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), t0));
+    const float tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), t1));
+    return tn <= tf;
+  }
+};
+
+// Conservative [a, b] of the ray parameters at which particle (c, r) can hold a point of the ray
+// (sphere inflated by 2^-10 r + eps, interval by eps); false when the ray misses it. Culling only:
+// fused steps round differently from the plain ones by far less than the slack.
+__device__ __forceinline__ bool sphere_span(float4 c, float3 o, float3 d, float eps, float& a, float& b) {
+  const float vx = c.x - o.x, vy = c.y - o.y, vz = c.z - o.z;
+  const float tc = fmaf(vz, d.z, fmaf(vy, d.y, vx * d.x));
+  const float wx = fmaf(-tc, d.x, vx), wy = fmaf(-tc, d.y, vy), wz = fmaf(-tc, d.z, vz);
+  const float h2 = fmaf(wz, wz, fmaf(wy, wy, wx * wx));
+  const float R = fmaf(c.w, 1.0f + 0x1p-10f, eps);
+  const float R2 = R * R;
+  if (h2 > R2) return false;
+  const float half = sqrtf(R2 - h2) + eps;
+  a = tc - half;
+  b = tc + half;
+  return true;
+}
+
 constexpr int kWarpStack = 8192;      // traversal stack entries per warp (global memory: a shared-memory
                                       // stack costs L1 capacity and measured slower)
 constexpr int kMaxSegBins = 64;       // bins per staged segment
