@@ -771,28 +771,36 @@ __device__ float4 raygen_generic(const RenderLaunch& L, uint32_t frame, int px, 
     tr.t = tenter + L.unit * r1;
     const bool from_entry = (L.flags & kFlagTrackFromEntry) != 0;
     const float t_start = (blue || from_entry) ? tr.t : ray.tmin;
-    track_fn(tr, ray, from_entry);
-    float4 albedo = tr.albedo;
-    float t = tr.t;
-    if (L.counters && count_lane) count_segment(L, ray, t_start, fminf(t, ray.tmax));
-    float vis = 1.0f;
-    if (albedo.w > 0.0f && L.ambient != 1.0f) {
-      Ray sr;
-      sr.o = make_float3(ray.o.x + ray.d.x * t, ray.o.y + ray.d.y * t, ray.o.z + ray.d.z * t);
-      sr.d = make_float3(L.light[0], L.light[1], L.light[2]);
-      sr.tmin = 0.0f;
-      sr.tmax = 10000.0f;
+    float4 albedo = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float t = 0.0f, vis = 1.0f, ts0 = 0.0f;
+    Ray cur = ray;
+    bool cur_from_entry = from_entry;
+    // the tracker has one call site: pass 0 tracks the primary ray, pass 1 the shadow ray (NEE,
+    // deviceCodeRBF.hlsl:288-314), so an inlined tracker exists once in the kernel
+    for (int pass = 0; pass < 2; ++pass) {
+      track_fn(tr, cur, cur_from_entry);
+      if (pass == 1) {
+        vis = 1.0f - tr.albedo.w;
+        if (L.counters && count_lane) count_segment(L, cur, fmaxf(ts0, 0.0f), fminf(tr.t, cur.tmax));
+        break;
+      }
+      albedo = tr.albedo;
+      t = tr.t;
+      if (L.counters && count_lane) count_segment(L, ray, t_start, fminf(t, ray.tmax));
+      if (!(albedo.w > 0.0f && L.ambient != 1.0f)) break;
+      cur.o = make_float3(ray.o.x + ray.d.x * t, ray.o.y + ray.d.y * t, ray.o.z + ray.d.z * t);
+      cur.d = make_float3(L.light[0], L.light[1], L.light[2]);
+      cur.tmin = 0.0f;
+      cur.tmax = 10000.0f;
       float ste, stx;
-      aabb_clip(sr.o, sr.d, lb, rt, sr.tmin, sr.tmax, ste, stx);
-      sr.tmax = stx;
+      aabb_clip(cur.o, cur.d, lb, rt, cur.tmin, cur.tmax, ste, stx);
+      cur.tmax = stx;
+      cur_from_entry = false;
       tr.albedo = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
       tr.lhs = 0.0f;
       tr.shadow = true;
       tr.t = blue ? -L.unit * r2 : 0.0f;
-      const float ts0 = tr.t;
-      track_fn(tr, sr, false);
-      vis = 1.0f - tr.albedo.w;
-      if (L.counters && count_lane) count_segment(L, sr, fmaxf(ts0, 0.0f), fminf(tr.t, sr.tmax));
+      ts0 = tr.t;
     }
     if (albedo.w == 1.0f) {
       color.x = (albedo.x * vis) * (1.0f - L.ambient) + albedo.x * L.ambient;
@@ -1533,9 +1541,9 @@ __device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t
   float noise = 0.0f;
   float4 c = raygen_generic<MODE == kWarpMarch ? 1 : 0>(
       L, (L.frame_id + k) & 0xffffu, px, py, noise, COUNT && lane == 0, [&](Tracker& tr, const Ray& r, bool from_entry) {
-        if (MODE == kWarpMarch) tr = track_march_warp<CAPW>(L, tr, r, stk);
-        else if (MODE == kWarpDelta) tr = track_delta_warp<CAPW, COUNT>(L, tr, r, from_entry, stk);
-        else tr = track_majorant_warp<CAPW, COUNT>(L, tr, r, stk);
+        if (MODE == kWarpMarch) track_march_warp_body<CAPW>(L, tr, r, buf, stk);
+        else if (MODE == kWarpDelta) track_delta_warp_body<CAPW, COUNT>(L, tr, r, from_entry, buf, stk);
+        else track_majorant_warp_body<CAPW, COUNT>(L, tr, r, buf, stk);
       });
   if (cost) c.w = (float)(clock64() - c0);
   if (lane == 0) {

@@ -388,6 +388,18 @@ def precision_timing(args, dev, stream):
         imgs[form] = img[..., :3].double()
     out["rmse_fp16_vs_fp32_same_stream"] = float(((imgs["fp16"] - imgs["fp32"]) ** 2).mean().sqrt())
     out["speedup_fp16"] = out["fp16"]["mrays_s"] / out["fp32"]["mrays_s"]
+    # per image against the converged FP64 oracle of the 256 x 256 centre crop (committed fixture
+    # made by tests/golden/make_config3_reference.py for this scene)
+    fx = os.path.join(ROOT, "tests", "golden", "config3_fp64_crop.npz")
+    if os.path.exists(fx):
+        ref = np.load(fx)
+        if int(ref["particles"]) == args.precision_particles and (int(ref["width"]), int(ref["height"])) == (W, H):
+            x0, x1, y0, y1 = (int(v) for v in ref["region"])
+            r64 = torch.from_numpy(ref["rgb"].astype(np.float64)).to(dev)
+            out["fp64_reference"] = {"spp": int(ref["spp"]), "crop": [x0, y0, x1 - x0, y1 - y0],
+                                     "source": "FP64 oracle (CPU), tests/golden/config3_fp64_crop.npz"}
+            for form in ("fp32", "fp16"):
+                out[form]["rmse_vs_fp64"] = float(((imgs[form][y0:y1, x0:x1] - r64) ** 2).mean().sqrt())
     ctx.close()
     return out
 
