@@ -106,3 +106,20 @@ def test_loop_cap_differentiable_form(ctx, aarbf_mod):
     ctx.render_diff_forward(views, w, h, img)
     ctx.sync()
     assert torch.equal(img, ref)
+
+
+def test_work_item_count_is_checked(ctx, orc, aarbf_mod):
+    """a launch whose width x height x spp (pixels padded to 8 x 4 tiles) exceeds the persistent
+    kernels' 32-bit work-item count is refused on the host, before any allocation or launch"""
+    from aarbf import scenes
+    sc, dom, scene = _scene(ctx, orc, aarbf_mod)
+    rp = scenes.native_params(scenes.orbit_camera(), 64, 64, float(sc.radii.max()), 0.002, 200.0, dom, spp=2,
+                              majorant=True, bin_length=0.004)
+    small = ctx.device_alloc(1 << 16)
+    try:
+        with pytest.raises(aarbf_mod.AarbfError) as ei:
+            ctx.render(rp, 65536, 65536, small, small)  # 2^33 samples
+        assert ei.value.status == 1  # AARBF_ERR_INVALID_ARGUMENT
+        ctx.sync()  # nothing was launched: no device status either
+    finally:
+        ctx.device_free(small)
