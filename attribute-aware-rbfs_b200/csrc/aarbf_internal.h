@@ -251,6 +251,7 @@ struct aarbf_ctx {
   bool built = false;
   uint64_t built_n = 0;          // particle count and radii presence of the last aarbf_build
   bool built_has_radii = false;
+  bool has_topology = false;     // the last aarbf_build completed: its BVH topology can be refit
   float root_box_host[6] = {0, 0, 0, 0, 0, 0};
   // transfer functions
   aarbf::DevBuf tf_color, tf_radius, tf_density;

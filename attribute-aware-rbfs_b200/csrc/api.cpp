@@ -583,6 +583,7 @@ aarbf_status aarbf_build(aarbf_ctx* ctx, float rbf_radius, uint32_t ppl, void* s
   ctx->ppl = ppl;
   ctx->rbf_radius = rbf_radius;
   ctx->nleaves = (uint32_t)((n + ppl - 1) / ppl);
+  ctx->has_topology = false;
   // domain: the caller's space-time box, else this frame's own bounds
   float dom[8];
   if (ctx->has_domain) {
@@ -629,6 +630,7 @@ aarbf_status aarbf_build(aarbf_ctx* ctx, float rbf_radius, uint32_t ppl, void* s
   ctx->built_has_radii = ctx->has_radii;
   aarbf_status s = run_refit(ctx, st);
   if (s != AARBF_OK) return s;
+  ctx->has_topology = true;
   if (!n)
     for (int a = 0; a < 6; ++a) ctx->root_box_host[a] = NAN;
   return AARBF_OK;
@@ -637,7 +639,9 @@ aarbf_status aarbf_build(aarbf_ctx* ctx, float rbf_radius, uint32_t ppl, void* s
 
 aarbf_status aarbf_refit_frame(aarbf_ctx* ctx, int keep_order, void* stream) {
   if (!ctx) return AARBF_ERR_INVALID_ARGUMENT;
-  if (!ctx->built || !ctx->nodes.ptr) return fail(ctx, AARBF_ERR_NOT_READY, "refit_frame before build");
+  // a new frame clears `built` (the scene is stale until refit); the topology of the last
+  // completed aarbf_build is what this call needs
+  if (!ctx->has_topology || !ctx->nodes.ptr) return fail(ctx, AARBF_ERR_NOT_READY, "refit_frame before build");
   if (ctx->n != ctx->built_n || ctx->has_radii != ctx->built_has_radii)
     return fail(ctx, AARBF_ERR_INVALID_ARGUMENT,
                 "refit_frame needs a frame of the built particle count (and radii iff the build had them); "

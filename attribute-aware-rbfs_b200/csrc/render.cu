@@ -1541,9 +1541,9 @@ __device__ __forceinline__ void render_warp_item(const RenderLaunch& L, uint32_t
   float noise = 0.0f;
   float4 c = raygen_generic<MODE == kWarpMarch ? 1 : 0>(
       L, (L.frame_id + k) & 0xffffu, px, py, noise, COUNT && lane == 0, [&](Tracker& tr, const Ray& r, bool from_entry) {
-        if (MODE == kWarpMarch) track_march_warp_body<CAPW>(L, tr, r, buf, stk);
-        else if (MODE == kWarpDelta) track_delta_warp_body<CAPW, COUNT>(L, tr, r, from_entry, buf, stk);
-        else track_majorant_warp_body<CAPW, COUNT>(L, tr, r, buf, stk);
+        if (MODE == kWarpMarch) tr = track_march_warp<CAPW>(L, tr, r, stk);
+        else if (MODE == kWarpDelta) tr = track_delta_warp<CAPW, COUNT>(L, tr, r, from_entry, stk);
+        else tr = track_majorant_warp<CAPW, COUNT>(L, tr, r, stk);
       });
   if (cost) c.w = (float)(clock64() - c0);
   if (lane == 0) {

@@ -325,6 +325,8 @@ def params_from(rp, noise=None):
     p.density_scale = getattr(rp, "density_scale", 0.0)
     p.bin_length = getattr(rp, "bin_length", 0.0)
     if noise is not None:
+        noise = np.ascontiguousarray(noise, np.uint8)
         p.noise = noise.ctypes.data
         p.noise_h, p.noise_w = noise.shape[0], noise.shape[1]
+        p._noise_keepalive = noise  # p.noise points into this array: it lives as long as p
     return p

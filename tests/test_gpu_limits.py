@@ -71,7 +71,8 @@ def test_loop_cap_reports_device_limit(ctx, orc, aarbf_mod, kind):
     img = _render(ctx, rp, w, h, splat)
     ctx.sync()
     got = img.cpu().numpy()
-    p = orc.params_from(rp, noise=aarbf_mod.generate_noise_atlas())
+    atlas = aarbf_mod.generate_noise_atlas()
+    p = orc.params_from(rp, noise=atlas)
     want = scene.render_splat(p, w, h) if splat else scene.render(p, w, h)[1]
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
     assert not torch.isnan(img).any()
