@@ -1177,12 +1177,10 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
         continue;
       }
     }
-    // [b0, b1) and its halves: path bit l set = the interval at level l + 1 is the upper half;
-    // a pending upper half is replayed from [b0, b1) by the same midpoint operations, so its
-    // floats are those a stack of pending intervals would hold
     float lo = b0, hi = b1;
-    int depth = 0;
-    uint32_t path = 0;
+    int depth = 0, np = 0;
+    float pend_hi[kSplitDepth];
+    int pend_depth[kSplitDepth];
     for (;;) {
       wctr(ctr, kWcBins, 1);
       long long acc = direct ? warp_bin_sum_direct<CAPW>(L.s, ray, st.inv, lo, hi, buf, stk, L.status, ctr)
@@ -1191,6 +1189,9 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
       if (M > 0.0f) {
         float mid = lo + 0.5f * (hi - lo);
         if (M * (hi - lo) > kSplitSteps && depth < kSplitDepth && mid > lo && mid < hi) {
+          pend_hi[np] = hi;
+          pend_depth[np] = depth + 1;
+          ++np;
           hi = mid;
           depth += 1;
           continue;
@@ -1209,18 +1210,11 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
           if (t >= hi || t >= ray.tmax) break;
           float3 x = make_float3(ray.o.x + t * ray.d.x, ray.o.y + t * ray.d.y, ray.o.z + t * ray.d.z);
           Sample smp;
-          long long a0;
-          if (direct) {
-            smp = warp_point<CAPW>(L.s, x, buf, stk, L.status, ctr);
-            a0 = smp.a0;
-          } else {
-            bool any;
-            a0 = st.sample_density(L.s, k, t, x, any);
-          }
-          float D = (float)a0 * kFixInv;
+          if (direct) smp = warp_point<CAPW>(L.s, x, buf, stk, L.status, ctr);
+          else st.sample(L.s, k, t, x, smp);
+          float D = (float)smp.a0 * kFixInv;
           float sigma = D * scale;
           if (lcg_f(tr.rng) < sigma / M) {
-            if (!direct) st.sample(L.s, k, t, x, smp);  // the colour sums of the collision
             float3 c = sample_color(L, smp, D);
             tr.albedo = make_float4(c.x, c.y, c.z, 1.0f);
             tr.t = t;
@@ -1228,18 +1222,11 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
           }
         }
       }
-      const uint32_t pending = ~path & ((1u << depth) - 1u);  // lower halves whose upper half waits
-      if (!pending) break;
-      const int d = 31 - __clz(pending);
-      path = (path | (1u << d)) & ((2u << d) - 1u);
-      depth = d + 1;
-      lo = b0;
-      hi = b1;
-      for (int l = 0; l < depth; ++l) {
-        const float m = lo + 0.5f * (hi - lo);
-        if ((path >> l) & 1u) lo = m;
-        else hi = m;
-      }
+      if (np == 0) break;
+      lo = hi;
+      --np;
+      hi = pend_hi[np];
+      depth = pend_depth[np];
     }
     k += 1;
     t = b1;

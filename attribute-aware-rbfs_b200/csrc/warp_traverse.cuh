@@ -114,6 +114,8 @@ __device__ bool warp_traverse_wide(const SceneView& s, const WideNode* wide, uin
   const uint32_t lane = threadIdx.x & 31u, lt = lane_lt_mask();
   if (s.nleaves == 0) return true;
   const uint32_t ppl = s.ppl;
+  const bool pow2 = (ppl & (ppl - 1u)) == 0u;
+  const uint32_t shift = pow2 ? (uint32_t)__ffs((int)ppl) - 1u : 0u;
   if (s.root & kLeafBit) {
     for (uint32_t b = 0; b < ppl; b += 32) {
       uint32_t j = b + lane;
@@ -126,11 +128,8 @@ __device__ bool warp_traverse_wide(const SceneView& s, const WideNode* wide, uin
   int sp = 1;
   __syncwarp();
   const int cap = loop_bound(s.loop_cap, 1 << 24);
-  for (int guard = 0; sp > 0; ++guard) {
-    if (guard == cap) {  // truncated traversal: report it
-      if (lane == 0) atomicOr(status, kStatusLoopCap);
-      return false;
-    }
+  int guard = 0;
+  for (; sp > 0 && guard < cap; ++guard) {
     constexpr int kPer = 32 / kBvhWidth;
     const int take = sp < kPer ? sp : kPer;
     const int base = sp - take;
@@ -168,13 +167,18 @@ __device__ bool warp_traverse_wide(const SceneView& s, const WideNode* wide, uin
       bool v = j < total;
       uint64_t i = 0;
       if (v) {
-        uint32_t lf = leafbuf[j / ppl];
-        i = (uint64_t)lf * ppl + (j % ppl);
+        // leaf slot and offset of entry j: a shift and a mask when ppl is a power of two
+        const uint32_t q = pow2 ? j >> shift : j / ppl, r = pow2 ? j & (ppl - 1u) : j - q * ppl;
+        i = (uint64_t)leafbuf[q] * ppl + r;
         v = i < s.n;
       }
       if (!on_particle(v, (uint32_t)i)) return false;
     }
     __syncwarp();
+  }
+  if (sp > 0) {  // the iteration bound ran out: a truncated traversal, reported
+    if (lane == 0) atomicOr(status, kStatusLoopCap);
+    return false;
   }
   return true;
 }

@@ -68,6 +68,8 @@ def parse():
                     help="opacity below this is transparent (1/255: the 8-bit transfer-function resolution)")
     ap.add_argument("--cap", type=int, default=0,
                     help="staged candidates per ray: 256/512/1024 per warp (majorant), 0 = default")
+    ap.add_argument("--stage-bins", type=int, default=0,
+                    help="bins covered by a ray's first staging (1..64), 0 = default; tuning only")
     ap.add_argument("--plain-spp", type=int, default=1, help="spp of the plain-estimator comparison (0: skip)")
     ap.add_argument("--marching-spp", type=int, default=1, help="spp of the stochastic-marching variant")
     ap.add_argument("--taa-frames", type=int, default=64, help="frames of the jittered splat + TAA sequence")
@@ -194,6 +196,7 @@ def params_for(args, dom, rmax, frame_id=0, estimator=None, spp=None, camera_fn=
                               traversal=args.traversal, majorant=(est == "majorant"),
                               bin_length=args.bin * args.unit, camera_fn=camera_fn)
     rp.candidate_cap = args.cap if est == "majorant" else 0
+    rp.stage_bins = args.stage_bins
     return rp
 
 
@@ -296,7 +299,7 @@ def config_dict(args):
                           "delta tracking with the global majorant 1/unit + shadow ray"),
             "unit": args.unit, "density_scale": args.density_scale,
             "traversal": traversal_label(args), "particles_per_leaf": args.ppl,
-            "alpha_floor": args.alpha_floor, "candidate_cap": args.cap,
+            "alpha_floor": args.alpha_floor, "candidate_cap": args.cap, "stage_bins": args.stage_bins,
             "l2": "inputs_larger_than_l2", "parallelism": f"replicas{args.gpus}"}
 
 
