@@ -102,21 +102,24 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(args):
-    """DRAM bytes of one render launch of the default workload from the committed ncu summary
-    (profiles/render_traffic.txt), or None for any other workload."""
+def profiled_figures(args):
+    """ncu figures of the render kernel from the committed summary (profiles/render_traffic.txt):
+    DRAM bytes of one full launch of the default workload, L2 bytes per ray and the L2 throughput
+    of the small-case capture. Empty for any other workload."""
     default = (args.particles, args.width, args.height, args.spp, args.estimator) == (
         10_000_000, 1920, 1080, 16, "majorant")
+    out = {}
     if not default:
-        return None
+        return out
     try:
         with open(os.path.join(ROOT, "profiles", "render_traffic.txt")) as f:
             for line in f:
-                if line.startswith("dram_bytes_per_launch:"):
-                    return int(line.split(":", 1)[1])
+                if ":" in line and not line.startswith("#"):
+                    k, v = line.split(":", 1)
+                    out[k.strip()] = float(v)
     except Exception:
         pass
-    return None
+    return out
 
 
 class ClockSampler:
@@ -821,6 +824,10 @@ def main():
     launch_s = render_ms / 1e3 / max(timed_renders, 1)
     achieved = alg_bytes / launch_s / 1e9
     peak, peak_kind = measured_peak()
+    prof = profiled_figures(args)
+    traffic = int(prof["dram_bytes_per_launch"]) if "dram_bytes_per_launch" in prof else None
+    l2_bytes = int(prof["l2_bytes_per_ray"] * W * H * S) if "l2_bytes_per_ray" in prof else None
+    l2_frac = prof["lts_throughput_pct"] / 100 if "lts_throughput_pct" in prof else None
 
     # the plain estimator (global majorant 1/unit, the reference's tracking loop) on the same frame
     plain = None
@@ -905,7 +912,10 @@ def main():
             "data": "synthetic (seeded generator at the benchmark configuration's sizes and distributions)",
             "config": config_dict(args),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": profiled_traffic(args), "peak_kind": peak_kind,
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "l2_bytes_per_launch": l2_bytes, "l2_throughput_frac_small_case": l2_frac,
+                         "l2_note": "L2 bytes scaled by rays from the 480x270 2-spp capture of the same "
+                                    "kernel; the L2 throughput fraction is that capture's",
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "bytes_rule": "20 B x particles on traversed segments + 32 B x node visits + "
                                        "48 B x spp x W x H",
