@@ -183,6 +183,8 @@ cudaError_t splat_stack_words(size_t* words);
 // several scenes in one persistent launch of the ray-per-warp kernel (render.cu)
 struct BatchArgs {
   const RenderLaunch* launches;  // device: one launch block per scene
+  const RenderLaunch* host_launches;  // host copies of the launch blocks (kernel parameters)
+  const uint64_t* host_items;    // host: nscenes + 1 prefix sums of work items
   const uint64_t* item_ofs;      // device: nscenes + 1 prefix sums of work items
   const uint64_t* pix_ofs;       // device: nscenes + 1 prefix sums of pixels
   int nscenes;

@@ -789,6 +789,8 @@ struct aarbf_batch {
   bool fp16 = false;
   int blocks_per_sm = 0;  // launch shape (aarbf_batch_set_shape)
   int sample_major = 0;
+  std::vector<RenderLaunch> launches;  // host copies: the batched kernel takes them as parameters
+  std::vector<uint64_t> items;         // nscenes + 1 prefix sums of work items
   std::string last_error;
 };
 
@@ -857,6 +859,8 @@ aarbf_status aarbf_batch_create(aarbf_batch** out, aarbf_ctx* const* ctxs, const
     delete b;
     return cuda_fail(c0, e, "batch upload");
   }
+  b->launches = std::move(Ls);
+  b->items = std::move(items);
   *out = b;
   return AARBF_OK;
 }
@@ -874,6 +878,8 @@ aarbf_status aarbf_batch_render(aarbf_batch* b, int candidate_cap, void* stream)
   char* base = static_cast<char*>(b->dev.ptr);
   BatchArgs B;
   B.launches = reinterpret_cast<const RenderLaunch*>(base);
+  B.host_launches = b->launches.data();
+  B.host_items = b->items.data();
   B.item_ofs = reinterpret_cast<const uint64_t*>(base + off_items);
   B.pix_ofs = reinterpret_cast<const uint64_t*>(base + off_pix);
   B.nscenes = b->nscenes;

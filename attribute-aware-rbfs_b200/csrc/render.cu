@@ -15,6 +15,8 @@
 #include "aarbf_internal.h"
 #include "warp_traverse.cuh"
 
+#include <memory>
+
 // Compiled twice: AARBF_RENDER_NS = r32 reads the fp32 prepass records, r16 the packed FP16
 // storage form (AARBF_FP16_RECORDS); each build has no branch on the format in its hot loops.
 #ifndef AARBF_RENDER_NS
@@ -1555,30 +1557,44 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks) k_render_
   }
 }
 
-// Several scenes in one persistent launch: Ls[s] is scene s's launch block, items
-// [item_ofs[s], item_ofs[s + 1]) are its work items; warps take items from one counter.
+// Several scenes in one persistent launch. The scenes' launch blocks are one kernel parameter (as
+// the single-scene kernel's launch block is), so the raygen reads them from the constant bank and
+// the out-of-line trackers through a pointer into the parameter block, as in the single-scene
+// kernel; items [item_ofs[s], item_ofs[s + 1]) are scene s's work items, taken by the warps from
+// one counter. At most kBatchPerLaunch scenes per launch (the parameter block stays under the
+// 32 KB kernel-parameter limit); larger batches take several launches.
+constexpr int kBatchPerLaunch = 64;
+struct BatchLaunch {
+  RenderLaunch L[kBatchPerLaunch];
+  uint64_t item_ofs[kBatchPerLaunch + 1];
+  unsigned long long* work_counter;
+  uint32_t* warp_stacks;
+  int nscenes;
+  int sample_major;
+};
+static_assert(sizeof(BatchLaunch) <= 32000, "batched kernel parameters exceed the 32 KB limit");
+
 template <int CAPW>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks)
-    k_render_warp_batched(const RenderLaunch* __restrict__ Ls, const uint64_t* __restrict__ item_ofs, int nscenes,
-                          unsigned long long* work_counter, uint32_t* warp_stacks, int sample_major) {
+    k_render_warp_batched(const __grid_constant__ BatchLaunch P) {
   extern __shared__ __align__(16) char smem[];
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
   WarpBuf<CAPW>* buf = reinterpret_cast<WarpBuf<CAPW>*>(smem) + wib;
-  uint32_t* stk = warp_stacks + ((size_t)blockIdx.x * kWarpsPerBlock + wib) * kWarpStack;
-  const uint64_t total = item_ofs[nscenes];
+  uint32_t* stk = P.warp_stacks + ((size_t)blockIdx.x * kWarpsPerBlock + wib) * kWarpStack;
+  const uint64_t total = P.item_ofs[P.nscenes];
   for (;;) {
     unsigned long long item = 0;
-    if (lane == 0) item = atomicAdd(work_counter, 1ull);
+    if (lane == 0) item = atomicAdd(P.work_counter, 1ull);
     item = __shfl_sync(kFull, item, 0);
     if (item >= total) break;
-    int lo = 0, hi = nscenes;  // item_ofs[lo] <= item < item_ofs[hi]
+    int lo = 0, hi = P.nscenes;  // item_ofs[lo] <= item < item_ofs[hi]
     while (hi - lo > 1) {
       const int mid = (lo + hi) >> 1;
-      if (item_ofs[mid] <= item) lo = mid;
+      if (P.item_ofs[mid] <= item) lo = mid;
       else hi = mid;
     }
-    render_warp_item<CAPW, kWarpMajorant, false>(Ls[lo], (uint32_t)(item - item_ofs[lo]), buf, stk,
-                                                 sample_major != 0);
+    render_warp_item<CAPW, kWarpMajorant, false>(P.L[lo], (uint32_t)(item - P.item_ofs[lo]), buf, stk,
+                                                 P.sample_major != 0);
   }
 }
 
@@ -1786,12 +1802,21 @@ cudaError_t launch_warp_batched(const BatchArgs& B, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     if (sms * B.blocks_per_sm < blocks) blocks = sms * B.blocks_per_sm;
   }
-  e = cudaMemsetAsync(B.work_counter, 0, sizeof(unsigned long long), st);
-  if (e != cudaSuccess) return e;
-  k_render_warp_batched<CAPW><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(
-      B.launches, B.item_ofs, B.nscenes, B.work_counter, B.warp_stacks, B.sample_major);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  std::unique_ptr<BatchLaunch> P(new BatchLaunch());
+  P->work_counter = B.work_counter;
+  P->warp_stacks = B.warp_stacks;
+  P->sample_major = B.sample_major;
+  for (int c0 = 0; c0 < B.nscenes; c0 += kBatchPerLaunch) {
+    const int n = B.nscenes - c0 < kBatchPerLaunch ? B.nscenes - c0 : kBatchPerLaunch;
+    P->nscenes = n;
+    for (int i = 0; i < n; ++i) P->L[i] = B.host_launches[c0 + i];
+    for (int i = 0; i <= n; ++i) P->item_ofs[i] = B.host_items[c0 + i] - B.host_items[c0];
+    e = cudaMemsetAsync(B.work_counter, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    k_render_warp_batched<CAPW><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(*P);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   if (B.total_pixels)
     k_accumulate_batched<<<(unsigned)((B.total_pixels + 255) / 256), 256, 0, st>>>(B.launches, B.pix_ofs, B.nscenes);
   return cudaGetLastError();
