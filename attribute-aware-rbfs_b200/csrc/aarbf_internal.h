@@ -190,7 +190,7 @@ struct BatchArgs {
   int nscenes;
   uint64_t total_pixels;
   int candidate_cap;
-  unsigned long long* work_counter;
+  uint32_t* work_counters;        // device: 64 per-scene item counters (256 bytes)
   uint32_t* warp_stacks;
   bool fp16;                     // every scene is in the FP16 storage form
   int blocks_per_sm;             // resident blocks per SM (0 = the occupancy limit)

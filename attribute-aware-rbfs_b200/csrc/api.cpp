@@ -202,8 +202,10 @@ void fill_scene_view(const aarbf_ctx* ctx, const float* cam_pos, SceneView& s) {
   }
 }
 
+// context_planes: the per-sample colour planes and the noise plane are the context's (false: the
+// caller supplies them, as a batch does from its own memory)
 aarbf_status fill_launch(aarbf_ctx* ctx, const aarbf_params* p, int w, int h, float* accum, float* image,
-                         RenderLaunch& L) {
+                         RenderLaunch& L, bool context_planes = true) {
   if (!ctx->built) return fail(ctx, AARBF_ERR_NOT_READY, "render before aarbf_build");
   if (!p || w <= 0 || h <= 0) return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "bad render arguments");
   memset(&L, 0, sizeof(L));
@@ -268,10 +270,12 @@ aarbf_status fill_launch(aarbf_ctx* ctx, const aarbf_params* p, int w, int h, fl
     return fail(ctx, AARBF_ERR_INVALID_ARGUMENT, "majorant tracking needs bin_length > 0, density_scale >= 0");
   if (!ctx->work.ptr) CK(ctx->work.reserve(256), "work counter");
   L.work_counter = ctx->work.as<uint32_t>();
-  CK(ctx->samples.reserve(sizeof(float) * 4 * (size_t)w * (size_t)h * L.spp), "sample planes");
-  CK(ctx->noise_buf.reserve(sizeof(float) * (size_t)w * (size_t)h), "noise plane");
-  L.samples = ctx->samples.as<float4>();
-  L.noise_buf = ctx->noise_buf.as<float>();
+  if (context_planes) {
+    CK(ctx->samples.reserve(sizeof(float) * 4 * (size_t)w * (size_t)h * L.spp), "sample planes");
+    CK(ctx->noise_buf.reserve(sizeof(float) * (size_t)w * (size_t)h), "noise plane");
+    L.samples = ctx->samples.as<float4>();
+    L.noise_buf = ctx->noise_buf.as<float>();
+  }
   if (render_uses_warp_kernel(L)) {
     size_t words = 0;
     CK(render_warp_stack_words(&words), "warp kernel setup");
@@ -785,6 +789,7 @@ struct aarbf_batch {
   int nscenes = 0;
   uint64_t total_pixels = 0;
   DevBuf dev;           // launch blocks, item and pixel prefix sums, work counter
+  DevBuf planes;        // every scene's per-sample colour planes, then every scene's noise plane
   uint32_t* warp_stacks = nullptr;
   bool fp16 = false;
   int blocks_per_sm = 0;  // launch shape (aarbf_batch_set_shape)
@@ -827,7 +832,7 @@ aarbf_status aarbf_batch_create(aarbf_batch** out, aarbf_ctx* const* ctxs, const
       return fail(c0, AARBF_ERR_UNSUPPORTED, "batched rendering runs majorant tracking with AARBF_TRAVERSAL_AUTO");
     aarbf_params q = p;
     q.candidate_cap = 0;
-    aarbf_status s = fill_launch(ctx, &q, widths[i], heights[i], accums[i], images[i], Ls[(size_t)i]);
+    aarbf_status s = fill_launch(ctx, &q, widths[i], heights[i], accums[i], images[i], Ls[(size_t)i], false);
     if (s != AARBF_OK) {
       c0->last_error = ctx->last_error;
       return s;
@@ -846,16 +851,37 @@ aarbf_status aarbf_batch_create(aarbf_batch** out, aarbf_ctx* const* ctxs, const
   b->total_pixels = pix.back();
   b->warp_stacks = c0->warp_stacks.as<uint32_t>();
   b->fp16 = c0->built_fp16;
+  // the batch's own sample and noise planes: a context may appear more than once, and a single
+  // render through a context (which may reallocate the context's planes) leaves the batch intact
+  size_t sample_bytes = 0;
+  for (int i = 0; i < nscenes; ++i) sample_bytes += sizeof(float4) * (size_t)widths[i] * (size_t)heights[i] * Ls[(size_t)i].spp;
+  cudaError_t e = b->planes.reserve(sample_bytes + sizeof(float) * (size_t)b->total_pixels);
+  if (e != cudaSuccess) {
+    delete b;
+    return cuda_fail(c0, e, "batch sample planes");
+  }
+  {
+    float4* sp = b->planes.as<float4>();
+    float* np = reinterpret_cast<float*>(static_cast<char*>(b->planes.ptr) + sample_bytes);
+    for (int i = 0; i < nscenes; ++i) {
+      RenderLaunch& L = Ls[(size_t)i];
+      L.samples = sp;
+      L.noise_buf = np;
+      sp += (size_t)widths[i] * (size_t)heights[i] * L.spp;
+      np += (size_t)widths[i] * (size_t)heights[i];
+    }
+  }
   const size_t lb = sizeof(RenderLaunch) * (size_t)nscenes, ob = sizeof(uint64_t) * ((size_t)nscenes + 1);
   const size_t off_items = (lb + 255) / 256 * 256, off_pix = off_items + (ob + 255) / 256 * 256;
   const size_t off_ctr = off_pix + (ob + 255) / 256 * 256;
-  cudaError_t e = b->dev.reserve(off_ctr + 256);
+  e = b->dev.reserve(off_ctr + 256);
   if (e == cudaSuccess) e = cudaMemcpy(b->dev.ptr, Ls.data(), lb, cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(static_cast<char*>(b->dev.ptr) + off_items, items.data(), ob, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(static_cast<char*>(b->dev.ptr) + off_pix, pix.data(), ob, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     b->dev.release();
+    b->planes.release();
     delete b;
     return cuda_fail(c0, e, "batch upload");
   }
@@ -885,7 +911,7 @@ aarbf_status aarbf_batch_render(aarbf_batch* b, int candidate_cap, void* stream)
   B.nscenes = b->nscenes;
   B.total_pixels = b->total_pixels;
   B.candidate_cap = candidate_cap;
-  B.work_counter = reinterpret_cast<unsigned long long*>(base + off_ctr);
+  B.work_counters = reinterpret_cast<uint32_t*>(base + off_ctr);  // 256 bytes: 64 counters
   B.warp_stacks = b->warp_stacks;
   B.fp16 = b->fp16;
   B.blocks_per_sm = b->blocks_per_sm;
@@ -902,6 +928,7 @@ aarbf_status aarbf_batch_destroy(aarbf_batch* b) {
   if (!b) return AARBF_OK;
   cudaSetDevice(b->device);
   b->dev.release();
+  b->planes.release();
   delete b;
   return AARBF_OK;
 }

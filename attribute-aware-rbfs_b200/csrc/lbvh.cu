@@ -80,7 +80,7 @@ __global__ void k_karras(const uint64_t* __restrict__ keys, uint32_t ppl, uint32
     Node* nd = trees[t];
     nd[i].d.x = left;
     nd[i].d.y = right;
-    nd[i].d.w = 0u;
+    nd[i].d.w = (uint32_t)j;  // the other end of the node's leaf range [min(i, j), max(i, j)]
     if (i == 0) nd[0].d.z = 0xffffffffu;
     if (!(left & kLeafBit)) nd[left].d.z = (uint32_t)i;
     if (!(right & kLeafBit)) nd[right].d.z = (uint32_t)i;
@@ -116,10 +116,17 @@ __device__ __forceinline__ void nan_if_empty(float* lo, float* hi) {
 
 // one thread per leaf: GenRBFBounds (deviceCodeBounds.hlsl:45-81) and the traversal box, then
 // walk up the tree; the second child to arrive at an internal node computes both of its boxes.
-__global__ void k_refit(const float4* __restrict__ rec0, const float* __restrict__ rgeom, uint64_t n,
+constexpr int kRefitBlock = 256;  // threads (leaves) per refit block
+
+__global__ void __launch_bounds__(kRefitBlock) k_refit(const float4* __restrict__ rec0, const float* __restrict__ rgeom, uint64_t n,
                         uint32_t ppl, uint32_t nleaves, Node* nodes, Node* nodes_ref,
                         const uint32_t* __restrict__ leaf_parent, uint32_t* counters, float* __restrict__ leaf_box,
                         float* __restrict__ leaf_eff, float* __restrict__ root_box, uint32_t* status) {
+  // per inner node of this block's window: both children's boxes of both trees, arrival count
+  __shared__ float s_box[kRefitBlock * 24];
+  __shared__ uint32_t s_cnt[kRefitBlock];
+  s_cnt[threadIdx.x] = 0u;
+  __syncthreads();
   uint64_t l = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (l >= nleaves) return;
   const float inf = __int_as_float(0x7f800000);
@@ -156,6 +163,12 @@ __global__ void k_refit(const float4* __restrict__ rec0, const float* __restrict
     }
     return;
   }
+  // Climb. An inner node whose leaf range lies in this block's leaves [b0, b0 + blockDim) has
+  // index in that window too and only this block's threads arrive at it: those nodes meet in
+  // shared memory (block-scope fences, shared arrival counters). The first node reaching outside
+  // the window, and every ancestor of it, meets in global memory (device-scope fences).
+  const uint32_t b0 = blockIdx.x * blockDim.x;
+  bool local = true;
   uint32_t child = (uint32_t)l | kLeafBit;
   uint32_t parent = leaf_parent[l];
   for (int guard = 0; guard < 256; ++guard) {
@@ -164,13 +177,41 @@ __global__ void k_refit(const float4* __restrict__ rec0, const float* __restrict
     int slot = (pn->d.x == child) ? 0 : 1;
     write_slot(pn, slot, elo, ehi);
     write_slot(pr, slot, lo, hi);
-    // release the slot before the arrival count, acquire the sibling's slot after it
-    // (acquire-release fences: the message-passing pattern needs no sequentially consistent fence)
-    asm volatile("fence.acq_rel.gpu;" ::: "memory");
-    if (atomicAdd(counters + parent, 1u) == 0u) return;
-    asm volatile("fence.acq_rel.gpu;" ::: "memory");
-    read_union(pn, elo, ehi);
-    read_union(pr, lo, hi);
+    if (local) {
+      const uint32_t j = pn->d.w;
+      const uint32_t first = parent < j ? parent : j, last = parent < j ? j : parent;
+      local = first >= b0 && last < b0 + blockDim.x;
+    }
+    if (local) {
+      const uint32_t q = parent - b0;  // first <= parent <= last: inside the window
+      float* mine = s_box + q * 24u + (uint32_t)slot * 12u;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        mine[a] = elo[a];
+        mine[3 + a] = ehi[a];
+        mine[6 + a] = lo[a];
+        mine[9 + a] = hi[a];
+      }
+      __threadfence_block();
+      if (atomicAdd(s_cnt + q, 1u) == 0u) return;
+      __threadfence_block();
+      const float* other = s_box + q * 24u + (uint32_t)(1 - slot) * 12u;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        elo[a] = fminf(elo[a], other[a]);
+        ehi[a] = fmaxf(ehi[a], other[3 + a]);
+        lo[a] = fminf(lo[a], other[6 + a]);
+        hi[a] = fmaxf(hi[a], other[9 + a]);
+      }
+    } else {
+      // release the slot before the arrival count, acquire the sibling's slot after it
+      // (acquire-release fences: the message-passing pattern needs no sequentially consistent fence)
+      asm volatile("fence.acq_rel.gpu;" ::: "memory");
+      if (atomicAdd(counters + parent, 1u) == 0u) return;
+      asm volatile("fence.acq_rel.gpu;" ::: "memory");
+      read_union(pn, elo, ehi);
+      read_union(pr, lo, hi);
+    }
     uint32_t up = pn->d.z;
     if (up == 0xffffffffu) {
 #pragma unroll
@@ -287,7 +328,7 @@ cudaError_t launch_refit(const float4* rec0, const float* rgeom, uint64_t n, uin
     cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(uint32_t) * (nleaves - 1), st);
     if (e != cudaSuccess) return e;
   }
-  k_refit<<<blocks_for(nleaves, 256), 256, 0, st>>>(rec0, rgeom, n, ppl, nleaves, nodes, nodes_ref, leaf_parent,
+  k_refit<<<blocks_for(nleaves, kRefitBlock), kRefitBlock, 0, st>>>(rec0, rgeom, n, ppl, nleaves, nodes, nodes_ref, leaf_parent,
                                                    counters, leaf_box, leaf_eff, root_box, status);
   return cudaGetLastError();
 }

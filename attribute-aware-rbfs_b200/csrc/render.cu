@@ -1551,7 +1551,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks) k_render_
   for (;;) {
     uint32_t item = 0;
     if (lane == 0) item = atomicAdd(L.work_counter, 1u);
-    item = __shfl_sync(kFull, item, 0);
+    // broadcast by a warp reduction: its result is known warp-uniform, so the item's pixel and
+    // ray setup can use uniform registers
+    item = __reduce_max_sync(kFull, item);
     if (item >= total) break;
     render_warp_item<CAPW, MODE, COUNT>(L, item, buf, stk);
   }
@@ -1560,14 +1562,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks) k_render_
 // Several scenes in one persistent launch. The scenes' launch blocks are one kernel parameter (as
 // the single-scene kernel's launch block is), so the raygen reads them from the constant bank and
 // the out-of-line trackers through a pointer into the parameter block, as in the single-scene
-// kernel; items [item_ofs[s], item_ofs[s + 1]) are scene s's work items, taken by the warps from
-// one counter. At most kBatchPerLaunch scenes per launch (the parameter block stays under the
-// 32 KB kernel-parameter limit); larger batches take several launches.
+// kernel. Every warp walks the scenes in order and takes items of the current scene from that
+// scene's counter until they run out, then moves on to the next scene: no warp waits for a scene
+// to finish, and the scene index is a loop counter every lane agrees on (warp-uniform, like the
+// item, which is broadcast by a warp reduction), so scene fields are read with uniform addresses.
+// At most kBatchPerLaunch scenes per launch (the parameter block stays under the 32 KB
+// kernel-parameter limit); larger batches take several launches.
 constexpr int kBatchPerLaunch = 64;
 struct BatchLaunch {
   RenderLaunch L[kBatchPerLaunch];
-  uint64_t item_ofs[kBatchPerLaunch + 1];
-  unsigned long long* work_counter;
+  uint32_t items[kBatchPerLaunch];  // work items of each scene
+  uint32_t* counters;               // kBatchPerLaunch per-scene item counters, zeroed per launch
   uint32_t* warp_stacks;
   int nscenes;
   int sample_major;
@@ -1581,20 +1586,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks)
   const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
   WarpBuf<CAPW>* buf = reinterpret_cast<WarpBuf<CAPW>*>(smem) + wib;
   uint32_t* stk = P.warp_stacks + ((size_t)blockIdx.x * kWarpsPerBlock + wib) * kWarpStack;
-  const uint64_t total = P.item_ofs[P.nscenes];
-  for (;;) {
-    unsigned long long item = 0;
-    if (lane == 0) item = atomicAdd(P.work_counter, 1ull);
-    item = __shfl_sync(kFull, item, 0);
-    if (item >= total) break;
-    int lo = 0, hi = P.nscenes;  // item_ofs[lo] <= item < item_ofs[hi]
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (P.item_ofs[mid] <= item) lo = mid;
-      else hi = mid;
+  for (int s = 0; s < P.nscenes; ++s) {
+    const uint32_t total = P.items[s];
+    for (;;) {
+      uint32_t item = 0;
+      if (lane == 0) item = atomicAdd(P.counters + s, 1u);
+      item = __reduce_max_sync(kFull, item);
+      if (item >= total) break;
+      render_warp_item<CAPW, kWarpMajorant, false>(P.L[s], item, buf, stk, P.sample_major != 0);
     }
-    render_warp_item<CAPW, kWarpMajorant, false>(P.L[lo], (uint32_t)(item - P.item_ofs[lo]), buf, stk,
-                                                 P.sample_major != 0);
   }
 }
 
@@ -1803,15 +1803,17 @@ cudaError_t launch_warp_batched(const BatchArgs& B, cudaStream_t st) {
     if (sms * B.blocks_per_sm < blocks) blocks = sms * B.blocks_per_sm;
   }
   std::unique_ptr<BatchLaunch> P(new BatchLaunch());
-  P->work_counter = B.work_counter;
+  P->counters = B.work_counters;
   P->warp_stacks = B.warp_stacks;
   P->sample_major = B.sample_major;
   for (int c0 = 0; c0 < B.nscenes; c0 += kBatchPerLaunch) {
     const int n = B.nscenes - c0 < kBatchPerLaunch ? B.nscenes - c0 : kBatchPerLaunch;
     P->nscenes = n;
-    for (int i = 0; i < n; ++i) P->L[i] = B.host_launches[c0 + i];
-    for (int i = 0; i <= n; ++i) P->item_ofs[i] = B.host_items[c0 + i] - B.host_items[c0];
-    e = cudaMemsetAsync(B.work_counter, 0, sizeof(unsigned long long), st);
+    for (int i = 0; i < n; ++i) {
+      P->L[i] = B.host_launches[c0 + i];
+      P->items[i] = (uint32_t)(B.host_items[c0 + i + 1] - B.host_items[c0 + i]);  // < 2^32: fill_launch
+    }
+    e = cudaMemsetAsync(B.work_counters, 0, sizeof(uint32_t) * kBatchPerLaunch, st);
     if (e != cudaSuccess) return e;
     k_render_warp_batched<CAPW><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(*P);
     e = cudaGetLastError();

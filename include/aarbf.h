@@ -226,7 +226,11 @@ aarbf_status aarbf_set_storage(aarbf_ctx *ctx, int format);
  * (synchronous). aarbf_batch_render then only enqueues the two kernels on `stream`: it allocates
  * nothing and does not synchronise, so it can be called repeatedly or captured; candidate_cap
  * (0, 256, 512, 1024) picks the staging-buffer depth. Results equal aarbf_render of each scene.
- * The contexts must outlive the batch and not be rebuilt while it is used. */
+ * The batch holds its own per-sample colour planes, so one context may appear several times
+ * (other views of the same scene) and may render on its own between batch renders. The
+ * contexts must outlive the batch, and their scenes, transfer functions and noise atlases must
+ * not be rebuilt or replaced while it is used. Up to 64 scenes run in one persistent launch;
+ * larger batches take one launch per 64 scenes. */
 typedef struct aarbf_batch aarbf_batch;
 aarbf_status aarbf_batch_create(aarbf_batch **out, aarbf_ctx *const *ctxs, const aarbf_params *params,
                                 int nscenes, const int *widths, const int *heights,
