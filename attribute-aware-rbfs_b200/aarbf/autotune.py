@@ -2,7 +2,9 @@
 
 Every knob changes only speed, never results:
   - candidate_cap: staging-buffer depth of the ray-per-warp kernel (256, 512 or 1024 candidates);
-  - stage_bins: majorant bins covered by a ray's first staging (2, 4 or 8; later stagings double);
+  - stage_bins: majorant bins covered by a ray's first staging (2, 4, 8 or 16; later stagings double),
+    per scene (scene_plan: each scene's 1-spp render timed with each length) or one for the whole
+    batch (tune_batch);
   - blocks_per_sm: resident blocks of four warps per SM (6, 7 or the occupancy limit of 8), the
     block-level shape of the persistent launch;
   - sample_major: the ray order -- the work items of a batch run tile by tile with a tile's
@@ -19,7 +21,7 @@ from __future__ import annotations
 import copy
 
 CAPS = (256, 512, 1024)
-STAGE_BINS = (2, 4, 8)
+STAGE_BINS = (2, 4, 8, 16)
 BLOCKS_PER_SM = (6, 7, 0)
 SAMPLE_MAJOR = (False, True)
 
@@ -53,23 +55,54 @@ def scene_order(contexts, params, sizes, accums, images, stream=None):
     return sorted(range(len(cost)), key=lambda i: -cost[i])
 
 
-def tune_batch(contexts, params, sizes, accums, images, stream=None, reps: int = 1):
+def scene_plan(contexts, params, sizes, accums, images, stream=None):
+    """(order, stage_bins, cost): for every scene the first-staging length of STAGE_BINS whose 1-spp
+    render, timed on its own, is fastest; the scene indices longest first by that time x spp; and
+    the cost estimates (ms)"""
+    import torch
+    st = stream or torch.cuda.current_stream()
+    bins_of, cost = [], []
+    for c, p, (w, h), a, im in zip(contexts, params, sizes, accums, images):
+        best = None
+        for bins in STAGE_BINS:
+            q = copy.copy(p)
+            q.spp = 1
+            q.stage_bins = bins
+            c.render(q, w, h, a, im, stream=st.cuda_stream)  # warm-up
+            e0, e1 = _events()
+            e0.record(st)
+            c.render(q, w, h, a, im, stream=st.cuda_stream)
+            e1.record(st)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            if best is None or ms < best[0]:
+                best = (ms, bins)
+        bins_of.append(best[1])
+        cost.append(best[0] * max(int(p.spp), 1))
+    order = sorted(range(len(cost)), key=lambda i: -cost[i])
+    return order, bins_of, cost
+
+
+def tune_batch(contexts, params, sizes, accums, images, stream=None, reps: int = 1, stage_bins=STAGE_BINS):
     """(candidate_cap, stage_bins, {(cap, bins): ms}) of the fastest batched launch (tuned on these
-    parameters; the caller usually passes 1-spp proxies of its scenes). The blocks-per-SM and
-    ray-order choices are in tune_shape."""
+    parameters; the caller usually passes 1-spp proxies of its scenes). stage_bins: the lengths
+    tried for the whole batch, or None to keep each scene's own (then the returned stage_bins is
+    None). The blocks-per-SM and ray-order choices are in tune_shape."""
     import torch
 
     from . import Batch
-    key = signature(contexts, params, sizes)
+    key = (signature(contexts, params, sizes), stage_bins,
+           tuple(int(p.stage_bins) for p in params) if stage_bins is None else None)
     if key in _cache:
         return _cache[key]
     times = {}
     st = stream or torch.cuda.current_stream()
-    for bins in STAGE_BINS:
+    for bins in (stage_bins if stage_bins is not None else (None,)):
         ps = []
         for p in params:
             q = copy.copy(p)
-            q.stage_bins = bins
+            if bins is not None:
+                q.stage_bins = bins
             ps.append(q)
         b = Batch(contexts, ps, sizes, accums, images)
         for cap in CAPS:

@@ -185,7 +185,6 @@ struct BatchArgs {
   const RenderLaunch* launches;  // device: one launch block per scene
   const RenderLaunch* host_launches;  // host copies of the launch blocks (kernel parameters)
   const uint64_t* host_items;    // host: nscenes + 1 prefix sums of work items
-  const uint64_t* item_ofs;      // device: nscenes + 1 prefix sums of work items
   const uint64_t* pix_ofs;       // device: nscenes + 1 prefix sums of pixels
   int nscenes;
   uint64_t total_pixels;

@@ -799,6 +799,18 @@ struct aarbf_batch {
   std::string last_error;
 };
 
+// the batch's device block: launch blocks (read by the accumulation pass), pixel prefix sums,
+// 64 per-scene item counters
+struct BatchLayout {
+  size_t launch_bytes, pix_bytes, off_pix, off_ctr, bytes;
+  explicit BatchLayout(int nscenes)
+      : launch_bytes(sizeof(RenderLaunch) * (size_t)nscenes), pix_bytes(sizeof(uint64_t) * ((size_t)nscenes + 1)) {
+    off_pix = (launch_bytes + 255) / 256 * 256;
+    off_ctr = off_pix + (pix_bytes + 255) / 256 * 256;
+    bytes = off_ctr + 64 * sizeof(uint32_t);
+  }
+};
+
 aarbf_status aarbf_batch_set_shape(aarbf_batch* b, int blocks_per_sm, int sample_major) {
   if (!b) return AARBF_ERR_INVALID_ARGUMENT;
   if (blocks_per_sm < 0 || blocks_per_sm > 64 || (sample_major != 0 && sample_major != 1)) {
@@ -871,14 +883,11 @@ aarbf_status aarbf_batch_create(aarbf_batch** out, aarbf_ctx* const* ctxs, const
       np += (size_t)widths[i] * (size_t)heights[i];
     }
   }
-  const size_t lb = sizeof(RenderLaunch) * (size_t)nscenes, ob = sizeof(uint64_t) * ((size_t)nscenes + 1);
-  const size_t off_items = (lb + 255) / 256 * 256, off_pix = off_items + (ob + 255) / 256 * 256;
-  const size_t off_ctr = off_pix + (ob + 255) / 256 * 256;
-  e = b->dev.reserve(off_ctr + 256);
-  if (e == cudaSuccess) e = cudaMemcpy(b->dev.ptr, Ls.data(), lb, cudaMemcpyHostToDevice);
+  const BatchLayout lay(nscenes);
+  e = b->dev.reserve(lay.bytes);
+  if (e == cudaSuccess) e = cudaMemcpy(b->dev.ptr, Ls.data(), lay.launch_bytes, cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
-    e = cudaMemcpy(static_cast<char*>(b->dev.ptr) + off_items, items.data(), ob, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(static_cast<char*>(b->dev.ptr) + off_pix, pix.data(), ob, cudaMemcpyHostToDevice);
+    e = cudaMemcpy(static_cast<char*>(b->dev.ptr) + lay.off_pix, pix.data(), lay.pix_bytes, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     b->dev.release();
     b->planes.release();
@@ -898,20 +907,17 @@ aarbf_status aarbf_batch_render(aarbf_batch* b, int candidate_cap, void* stream)
     return AARBF_ERR_INVALID_ARGUMENT;
   }
   cudaSetDevice(b->device);
-  const size_t lb = sizeof(RenderLaunch) * (size_t)b->nscenes, ob = sizeof(uint64_t) * ((size_t)b->nscenes + 1);
-  const size_t off_items = (lb + 255) / 256 * 256, off_pix = off_items + (ob + 255) / 256 * 256;
-  const size_t off_ctr = off_pix + (ob + 255) / 256 * 256;
+  const BatchLayout lay(b->nscenes);
   char* base = static_cast<char*>(b->dev.ptr);
   BatchArgs B;
   B.launches = reinterpret_cast<const RenderLaunch*>(base);
   B.host_launches = b->launches.data();
   B.host_items = b->items.data();
-  B.item_ofs = reinterpret_cast<const uint64_t*>(base + off_items);
-  B.pix_ofs = reinterpret_cast<const uint64_t*>(base + off_pix);
+  B.pix_ofs = reinterpret_cast<const uint64_t*>(base + lay.off_pix);
   B.nscenes = b->nscenes;
   B.total_pixels = b->total_pixels;
   B.candidate_cap = candidate_cap;
-  B.work_counters = reinterpret_cast<uint32_t*>(base + off_ctr);  // 256 bytes: 64 counters
+  B.work_counters = reinterpret_cast<uint32_t*>(base + lay.off_ctr);
   B.warp_stacks = b->warp_stacks;
   B.fp16 = b->fp16;
   B.blocks_per_sm = b->blocks_per_sm;

@@ -1575,11 +1575,12 @@ struct BatchLaunch {
   uint32_t* counters;               // kBatchPerLaunch per-scene item counters, zeroed per launch
   uint32_t* warp_stacks;
   int nscenes;
-  int sample_major;
 };
 static_assert(sizeof(BatchLaunch) <= 32000, "batched kernel parameters exceed the 32 KB limit");
 
-template <int CAPW>
+// SMAJ: work items sample by sample over all tiles (a compile-time choice, as in the single-scene
+// kernel, so the item decode carries one form)
+template <int CAPW, bool SMAJ>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks)
     k_render_warp_batched(const __grid_constant__ BatchLaunch P) {
   extern __shared__ __align__(16) char smem[];
@@ -1593,7 +1594,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kWarpMinBlocks)
       if (lane == 0) item = atomicAdd(P.counters + s, 1u);
       item = __reduce_max_sync(kFull, item);
       if (item >= total) break;
-      render_warp_item<CAPW, kWarpMajorant, false>(P.L[s], item, buf, stk, P.sample_major != 0);
+      render_warp_item<CAPW, kWarpMajorant, false>(P.L[s], item, buf, stk, SMAJ);
     }
   }
 }
@@ -1733,7 +1734,8 @@ cudaError_t warp_grid(int* blocks) {
                    k_render_warp<CAPW, kWarpMarch, false>, k_render_warp<CAPW, kWarpMarch, true>,
                    k_render_warp<CAPW, kWarpDelta, false>, k_render_warp<CAPW, kWarpDelta, true>})
       if (e == cudaSuccess) e = cudaFuncSetAttribute(f, attr, smem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_render_warp_batched<CAPW>, attr, smem);
+    for (auto f : {k_render_warp_batched<CAPW, false>, k_render_warp_batched<CAPW, true>})
+      if (e == cudaSuccess) e = cudaFuncSetAttribute(f, attr, smem);
     int sms = 0, per_sm = 0;
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     for (auto f : {k_render_warp<CAPW, kWarpMajorant, false>, k_render_warp<CAPW, kWarpMarch, false>,
@@ -1805,7 +1807,6 @@ cudaError_t launch_warp_batched(const BatchArgs& B, cudaStream_t st) {
   std::unique_ptr<BatchLaunch> P(new BatchLaunch());
   P->counters = B.work_counters;
   P->warp_stacks = B.warp_stacks;
-  P->sample_major = B.sample_major;
   for (int c0 = 0; c0 < B.nscenes; c0 += kBatchPerLaunch) {
     const int n = B.nscenes - c0 < kBatchPerLaunch ? B.nscenes - c0 : kBatchPerLaunch;
     P->nscenes = n;
@@ -1815,7 +1816,8 @@ cudaError_t launch_warp_batched(const BatchArgs& B, cudaStream_t st) {
     }
     e = cudaMemsetAsync(B.work_counters, 0, sizeof(uint32_t) * kBatchPerLaunch, st);
     if (e != cudaSuccess) return e;
-    k_render_warp_batched<CAPW><<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(*P);
+    auto f = B.sample_major ? k_render_warp_batched<CAPW, true> : k_render_warp_batched<CAPW, false>;
+    f<<<blocks, kWarpsPerBlock * 32, sizeof(WarpBuf<CAPW>) * kWarpsPerBlock, st>>>(*P);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }

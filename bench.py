@@ -535,19 +535,30 @@ def batched_timing(args, dev, stream):
         q = copy.copy(p)
         q.spp = 1
         proxy.append(q)
-    order = autotune.scene_order(ctxs, params, sizes, accs, imgs, stream)  # longest first
+    # longest first, and each scene's own best first-staging length
+    order, scene_bins, _ = autotune.scene_plan(ctxs, params, sizes, accs, imgs, stream)
     o = lambda seq: [seq[i] for i in order]  # noqa: E731
+
+    def with_bins(ps, bins):
+        out = []
+        for p, b_ in zip(ps, bins):
+            q = copy.copy(p)
+            q.stage_bins = b_
+            out.append(q)
+        return out
+
+    # one staging length for the whole batch, or each scene's own: whichever runs the proxy faster
     cap, bins, table = autotune.tune_batch(o(ctxs), o(proxy), o(sizes), o(accs), o(imgs), stream)
-    tuned = []
-    for p in o(params):
-        q = copy.copy(p)
-        q.stage_bins = bins
-        tuned.append(q)
-    proxy_tuned = []
-    for p in o(proxy):
-        q = copy.copy(p)
-        q.stage_bins = bins
-        proxy_tuned.append(q)
+    own = o(scene_bins)
+    cap_s, _, table_s = autotune.tune_batch(o(ctxs), with_bins(o(proxy), own), o(sizes), o(accs), o(imgs), stream,
+                                            stage_bins=None)
+    if min(table_s.values()) < min(table.values()):
+        cap, bins_list, bins = cap_s, own, "per scene"
+        table.update({(c_, "own"): v for (c_, _), v in table_s.items()})
+    else:
+        bins_list = [bins] * len(own)
+    tuned = with_bins(o(params), bins_list)
+    proxy_tuned = with_bins(o(proxy), bins_list)
     pb = aarbf.Batch(o(ctxs), proxy_tuned, o(sizes), o(accs), o(imgs))
     bps, smaj, shape_table = autotune.tune_shape(pb, cap, stream)
     pb.close()
@@ -602,9 +613,11 @@ def batched_timing(args, dev, stream):
             "sequential_ms": t_seq, "sequential_mrays_s": rays / t_seq / 1e3,
             "batched_direct_ms": t_direct, "batched_graph_ms": t_graph, "batched_mrays_s": rays / t_graph / 1e3,
             "speedup_vs_sequential": t_seq / t_graph, "images_identical": bool(same),
-            "autotuned": {"candidate_cap": cap, "stage_bins": bins, "blocks_per_sm": bps or "occupancy limit",
+            "autotuned": {"candidate_cap": cap, "stage_bins": bins,
+                          "scene_stage_bins": {str(b_): bins_list.count(b_) for b_ in sorted(set(bins_list))},
+                          "blocks_per_sm": bps or "occupancy limit",
                           "ray_order": "sample-major" if smaj else "tile-major",
-                          "scene_order": "longest first (1-spp proxy time x spp)",
+                          "scene_order": "longest first (1-spp proxy time at the scene's best staging length x spp)",
                           "proxy_ms": {f"{k[0]}/{k[1]}": round(v, 3) for k, v in table.items()},
                           "shape_proxy_ms": {f"{k[0]}/{int(k[1])}": round(v, 3) for k, v in shape_table.items()}},
             "plain_estimator_mrays_s": pr / t_plain / 1e3, "plain_sample": "first 8 scenes, 1 spp",

@@ -62,6 +62,27 @@ def test_batched_matches_single_renders(aarbf_mod, orc):
     with pytest.raises(aarbf_mod.AarbfError):
         b.set_shape(-1, False)
     b.set_shape(0, False)
+    # the autotuner's plan (longest first, each scene's own first-staging length): the same bits
+    import copy
+    from aarbf import autotune
+    order, bins, cost = autotune.scene_plan([c for c, _, _, _ in items], [p for _, p, _, _ in items],
+                                            [s for _, _, s, _ in items], accs, imgs)
+    assert sorted(order) == list(range(len(items))) and all(x in autotune.STAGE_BINS for x in bins)
+    assert all(cost[order[k]] >= cost[order[k + 1]] for k in range(len(order) - 1))
+    planned = []
+    for i in order:
+        q = copy.copy(items[i][1])
+        q.stage_bins = bins[i]
+        planned.append(q)
+    for a in accs:
+        a.zero_()
+    bp = aarbf_mod.Batch([items[i][0] for i in order], planned, [items[i][2] for i in order],
+                         [accs[i] for i in order], [imgs[i] for i in order])
+    bp.render(0)
+    torch.cuda.synchronize()
+    for (ra, ri), i in zip(ref, imgs):
+        assert np.array_equal(i.cpu().numpy().view(np.uint32), ri.view(np.uint32))
+    bp.close()
     # the same launch replayed from a CUDA graph
     st = torch.cuda.Stream()
     with torch.cuda.stream(st):
