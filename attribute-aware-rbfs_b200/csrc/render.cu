@@ -1068,6 +1068,21 @@ struct WarpStager {
   }
 };
 
+// Length of a ray's next staging after one of nb bins that staged n candidates: twice as long
+// (at most kMaxSegBins, the size of the per-bin list arrays), but no longer than this staging's
+// candidate density predicts fills half the buffer, so a dense run of bins is not staged long
+// enough to overflow and be staged again. Only the cost depends on it: a bin's candidates are
+// the same whatever segment it was staged with. With nb in [1, kMaxSegBins] the result is too.
+template <int CAPW>
+__device__ __forceinline__ int next_stage_bins(int nb, int n) {
+  int next = 2 * nb < kMaxSegBins ? 2 * nb : kMaxSegBins;
+  if (n > 0) {
+    const int fit = (CAPW * nb) / (2 * n);
+    next = fit < next ? (fit > 1 ? fit : 1) : next;
+  }
+  return next;
+}
+
 // direct (unbuffered) majorant sum of one bin; out of line (rare path, instruction-cache footprint)
 template <int CAPW>
 __device__ __noinline__ long long warp_bin_sum_direct(const SceneView& s, const Ray ray, const float3 inv, float lo,
@@ -1151,7 +1166,7 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
       for (;;) {
         if (st.stage(L.s, ray, k, nb, t0, Lb, L.status)) {
           seg_end = k + nb;
-          if (nb < kMaxSegBins) nb *= 2;
+          nb = next_stage_bins<CAPW>(nb, st.ncand);
           break;
         }
         nb >>= 1;
@@ -1287,7 +1302,7 @@ __device__ __forceinline__ void track_delta_warp_body(const RenderLaunch& L, Tra
         if (st.stage(L.s, ray, kb, nb, t0, Lb, L.status)) {
           seg_begin = kb;
           seg_end = kb + nb;
-          if (nb < kMaxSegBins) nb *= 2;
+          nb = next_stage_bins<CAPW>(nb, st.ncand);
           break;
         }
         nb >>= 1;

@@ -266,7 +266,7 @@ def test_render_marching_native_dense(ctx, orc, aarbf_mod, traversal):
 
 
 @pytest.mark.parametrize("traversal", [0, 2])
-@pytest.mark.parametrize("cap,bins", [(256, 0), (1024, 64)])
+@pytest.mark.parametrize("cap,bins", [(256, 0), (1024, 64), (256, 5), (512, 48)])
 def test_render_delta_native_dense(ctx, orc, aarbf_mod, traversal, cap, bins):
     """the reference's delta tracking (global majorant 1/unit, native density) through dense
     clusters: the warp tracker's stagings overflow and fall back to shorter runs and direct warp
@@ -325,6 +325,27 @@ def test_render_majorant_tracking(ctx, orc, aarbf_mod, n, ppl, bins, scale, floo
     assert_radiance(gi, oi, "image")
     assert_radiance(ga, oa, "accum")
     assert (oi[..., :3] > 0).mean() > 0.01  # the view is not empty
+
+
+@pytest.mark.parametrize("stage_bins", [1, 3, 48, 64])
+def test_render_majorant_stage_lengths(ctx, orc, aarbf_mod, stage_bins):
+    """the warp tracker's first staging length (any of 1..64; later stagings adapt to the staged
+    candidate density and never exceed the 64-bin lists) changes no bit"""
+    from aarbf import scenes
+    sc = scenes.config_clusters(200_000, clusters=8, seed=6)
+    cm, rm, dm = scenes.tf_linear_ramp()
+    dom = orc.domain([sc.xyzw])
+    w, h = 40, 30
+    rp = scenes.native_params(scenes.orbit_camera(), w, h, float(sc.radii.max()), 0.002, 200.0, dom, spp=2,
+                              majorant=True, bin_length=8 * 0.002)
+    rp.stage_bins = stage_bins
+    scene, *_ = setup_both(ctx, orc, aarbf_mod, sc.xyzw, sc.radii, 1, rp.rbf_radius, tf32=(cm, rm, dm),
+                           alpha_floor=1 / 255)
+    ga, gi = gpu_render(ctx, rp, w, h)
+    oa, oi = scene.render(orc.params_from(rp), w, h)
+    assert_radiance(gi, oi, "image")
+    assert_radiance(ga, oa, "accum")
+    assert (oi[..., :3] > 0).mean() > 0.01
 
 
 def test_kernel_timing(ctx, orc, aarbf_mod):
