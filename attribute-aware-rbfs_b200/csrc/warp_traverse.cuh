@@ -80,17 +80,19 @@ __device__ __forceinline__ uint32_t lane_lt_mask() {
   return m;
 }
 
+// Exact warp sums (every lane gets the total). A 64-bit value is cut into limbs of 26, 26 and 12
+// bits whose 32-lane sums fit 32 bits, summed by the warp-reduce instruction and put back
+// together modulo 2^64: the same integer as a shuffle tree, in three reductions instead of five
+// rounds of two shuffles and an add.
 __device__ __forceinline__ long long warp_sum(long long v) {
-#pragma unroll
-  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-  return v;
+  const unsigned long long u = (unsigned long long)v;
+  const unsigned long long s0 = __reduce_add_sync(kFull, (unsigned)(u & 0x3ffffffull));
+  const unsigned long long s1 = __reduce_add_sync(kFull, (unsigned)((u >> 26) & 0x3ffffffull));
+  const unsigned long long s2 = __reduce_add_sync(kFull, (unsigned)(u >> 52));
+  return (long long)(s0 + (s1 << 26) + (s2 << 52));
 }
 
-__device__ __forceinline__ int warp_sum(int v) {
-#pragma unroll
-  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-  return v;
-}
+__device__ __forceinline__ int warp_sum(int v) { return __reduce_add_sync(kFull, v); }
 
 // warp-kernel count-mode slots (lane 0 adds warp-uniform values)
 enum { kWcSteps = 2, kWcStages = 3, kWcOverflows = 4, kWcDirect = 5, kWcCands = 6, kWcBins = 7,
