@@ -2,7 +2,7 @@
 
 Every knob changes only speed, never results:
   - candidate_cap: staging-buffer depth of the ray-per-warp kernel (256, 512 or 1024 candidates);
-  - stage_bins: majorant bins covered by a ray's first staging (2, 4, 8 or 16; later stagings double),
+  - stage_bins: majorant bins covered by a ray's first staging (2, 4, 8, 16 or 32; later stagings adapt),
     per scene (scene_plan: each scene's 1-spp render timed with each length) or one for the whole
     batch (tune_batch);
   - blocks_per_sm: resident blocks of four warps per SM (6, 7 or the occupancy limit of 8), the
@@ -21,7 +21,7 @@ from __future__ import annotations
 import copy
 
 CAPS = (256, 512, 1024)
-STAGE_BINS = (2, 4, 8, 16)
+STAGE_BINS = (2, 4, 8, 16, 32)
 BLOCKS_PER_SM = (6, 7, 0)
 SAMPLE_MAJOR = (False, True)
 

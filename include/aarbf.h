@@ -91,7 +91,9 @@ typedef struct aarbf_params {
                                or 256, 512 or 1024 per warp for the warp kernel (0 = 256);
                                tuning only, results are identical for every value */
   int32_t stage_bins;       /* bins staged by the first traversal of a ray (1..64; 0 = 4 for the
-                               warp kernel, 16 per thread; later stagings double up to 64); the
+                               warp kernel, 16 per thread; later stagings double, the warp
+                               kernel's at most to 64 bins and to half a buffer of candidates at
+                               the last staging's density); the
                                bins are bin_length long (16 units when bin_length is 0 and majorant
                                tracking is off); tuning only */
   uint32_t loop_cap;        /* 0 = the built-in iteration bounds of the device loops (the
