@@ -1146,9 +1146,8 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
   int seg_end = 0;
   int nb = L.stage_bins;
   bool direct = false;
-  const int cap = loop_bound(L.s.loop_cap, 1 << 26);
-  int guard = 0;
-  for (; guard < cap; ++guard) {
+  int budget = loop_bound(L.s.loop_cap, 1 << 26);  // iterations left
+  for (; budget > 0; --budget) {
     float b0 = t0 + (float)k * Lb;
     float b1 = t0 + (float)(k + 1) * Lb;
     if (!(b0 < ray.tmax) || !(b1 > b0)) break;
@@ -1248,7 +1247,7 @@ __device__ __forceinline__ void track_majorant_warp_body(const RenderLaunch& L, 
     k += 1;
     t = b1;
   }
-  if (guard == cap && (threadIdx.x & 31u) == 0) atomicOr(L.status, kStatusLoopCap);
+  if (budget == 0 && (threadIdx.x & 31u) == 0) atomicOr(L.status, kStatusLoopCap);
   tr.t = t;
 }
 

@@ -129,9 +129,7 @@ __device__ bool warp_traverse_wide(const SceneView& s, const WideNode* wide, uin
   if (lane == 0) stk[0] = s.root;
   int sp = 1;
   __syncwarp();
-  const int cap = loop_bound(s.loop_cap, 1 << 24);
-  int guard = 0;
-  for (; sp > 0 && guard < cap; ++guard) {
+  for (int budget = loop_bound(s.loop_cap, 1 << 24); sp > 0 && budget > 0; --budget) {
     constexpr int kPer = 32 / kBvhWidth;
     const int take = sp < kPer ? sp : kPer;
     const int base = sp - take;
