@@ -85,8 +85,8 @@ struct SceneView {
   int per_particle_radius;
   uint32_t loop_cap;  // 0, or a lower iteration bound for every device loop (loop_bound)
   // FP16 storage form (null in the fp32 form): packed records the tracking kernels read
-  const uint2* posq;     // FP16 offsets x, y, z from the run origin, FP16 a^3
-  const uint2* colq;     // FP16 rgb^2.2 a^3
+  const uint2* posq;     // FP16 offsets x, y, z from the run origin, FP16 radius rounded up (culling)
+  const uint2* colq;     // FP16 rgb^2.2 a^3 and a^3
   const float4* origin;  // fp32 origin of every run of 256 particles
   const float* reval;    // fp32 r_eval
 };

@@ -5,8 +5,9 @@
 // and the per-particle weights a^3 and rgb^2.2 a^3 are rounded to FP16; radii stay fp32. The
 // rounded values are also written back into the fp32 arrays (sorted particles, prepass records),
 // so every other kernel, the BVH and the oracle see exactly what the FP16 records decode to.
-// The tracking kernels read the packed records instead: 8 bytes of position + a^3, 4 bytes of
-// radius and, for particles that contribute, 8 bytes of colour weights.
+// The tracking kernels read the packed records instead: 8 bytes of position + the radius rounded
+// up to FP16 (what the staging test reads: a conservative sphere), the fp32 radius (what the
+// density evaluation reads) and 8 bytes of a^3 + colour weights.
 #include <cuda_fp16.h>
 
 #include "aarbf_internal.h"
@@ -48,7 +49,7 @@ __global__ void __launch_bounds__(kRun) k_quantize_positions(float4* __restrict_
   if (!v) return;
   const uint32_t hx = hbits(p.x - ox), hy = hbits(p.y - oy), hz = hbits(p.z - oz), hw = hbits(p.w);
   xyzw[i] = make_float4(ox + hval(hx), oy + hval(hy), oz + hval(hz), hval(hw));
-  posq[i] = make_uint2(hx | (hy << 16), hz);  // the high half of .y receives a^3 later
+  posq[i] = make_uint2(hx | (hy << 16), hz);  // the high half of .y receives the culling radius later
 }
 
 __global__ void k_quantize_weights(float4* __restrict__ w4, const float4* __restrict__ rec0, uint64_t n,
@@ -59,9 +60,11 @@ __global__ void k_quantize_weights(float4* __restrict__ w4, const float4* __rest
   const uint32_t a = hbits(w.x), r = hbits(w.y), g = hbits(w.z), b = hbits(w.w);
   w4[i] = make_float4(hval(a), hval(r), hval(g), hval(b));
   const uint2 q = posq[i];
-  posq[i] = make_uint2(q.x, (q.y & 0xffffu) | (a << 16));
-  colq[i] = make_uint2(r | (g << 16), b);
-  reval[i] = rec0[i].w;
+  const float re = rec0[i].w;
+  const uint32_t rc = (uint32_t)__half_as_ushort(__float2half_ru(re));  // rounded up: culling only
+  posq[i] = make_uint2(q.x, (q.y & 0xffffu) | (rc << 16));
+  colq[i] = make_uint2(r | (g << 16), b | (a << 16));
+  reval[i] = re;
 }
 
 }  // namespace

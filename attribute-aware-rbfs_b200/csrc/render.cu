@@ -54,14 +54,24 @@ __device__ __forceinline__ float4 part_rec(const SceneView& s, uint32_t i) {
                      __ldg(s.reval + i));
 }
 
-__device__ __forceinline__ float part_a3(const SceneView& s, uint32_t i) { return hval16(__ldg(&s.posq[i].y) >> 16); }
+// the staging test's record: the position and the FP16 radius rounded up, so the staged spans
+// are a superset of the exact ones (the sums evaluate every candidate with the fp32 radius)
+__device__ __forceinline__ float4 part_cull(const SceneView& s, uint32_t i) {
+  const uint2 q = __ldg(s.posq + i);
+  const float4 o = __ldg(s.origin + (i >> 8));
+  return make_float4(o.x + hval16(q.x & 0xffffu), o.y + hval16(q.x >> 16), o.z + hval16(q.y & 0xffffu),
+                     hval16(q.y >> 16));
+}
+
+__device__ __forceinline__ float part_a3(const SceneView& s, uint32_t i) { return hval16(__ldg(&s.colq[i].y) >> 16); }
 
 __device__ __forceinline__ float4 part_w(const SceneView& s, uint32_t i) {
   const uint2 c = __ldg(s.colq + i);
-  return make_float4(part_a3(s, i), hval16(c.x & 0xffffu), hval16(c.x >> 16), hval16(c.y & 0xffffu));
+  return make_float4(hval16(c.y >> 16), hval16(c.x & 0xffffu), hval16(c.x >> 16), hval16(c.y & 0xffffu));
 }
 #else
 __device__ __forceinline__ float4 part_rec(const SceneView& s, uint32_t i) { return __ldg(s.rec0 + i); }
+__device__ __forceinline__ float4 part_cull(const SceneView& s, uint32_t i) { return part_rec(s, i); }
 __device__ __forceinline__ float part_a3(const SceneView& s, uint32_t i) { return __ldg(&s.w4[i].x); }
 __device__ __forceinline__ float4 part_w(const SceneView& s, uint32_t i) { return __ldg(s.w4 + i); }
 #endif
@@ -925,7 +935,7 @@ struct WarpStager {
           bool keep = false;
           float a = 0.0f, b = 0.0f;
           if (v) {
-            const float4 r = part_rec(s, i);
+            const float4 r = part_cull(s, i);
             if (r.w > 0.0f && sphere_span(r, ray.o, ray.d, eps, a, b)) keep = !(b < ts || a > te);
           }
           const uint32_t m = __ballot_sync(kFull, keep);
@@ -1365,7 +1375,7 @@ __device__ bool stage_segment(const SceneView& s, const Ray& ray, float3 inv, fl
         bool keep = false;
         float a = 0.0f, b = 0.0f;
         if (v) {
-          const float4 r = part_rec(s, i);
+          const float4 r = part_cull(s, i);
           if (r.w > 0.0f && sphere_span(r, ray.o, ray.d, eps, a, b)) keep = !(b < ta || a > tb);
         }
         const uint32_t m = __ballot_sync(kFull, keep);
